@@ -1,0 +1,317 @@
+// Oracle C ABI for the Python test harness (ctypes). TEST INFRASTRUCTURE ONLY: the parity tests,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg load this library as the checker; the
+// product never does.
+//
+// gro_trace_* mirror the reference's CPU entry points: GeodesicTracer::trace
+// (crates/gravlume-reference/src/geodesic.rs:53-62), ObservationTracer::trace
+// (observation.rs:189-231) and the ordered rayon batch GeodesicBatch::trace_ordered
+// (batch.rs:31-43), here as a std::thread pool that writes each outcome at its input index.
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <vector>
+
+#include "oracle_tracer.hpp"
+
+using namespace gro;
+
+template <class F>
+static void parallel_for(int64_t n, int threads, F&& body) {
+  if (threads <= 1 || n <= 1) {
+    for (int64_t i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::atomic<int64_t> next{0};
+  std::vector<std::thread> pool;
+  const int t = int(std::min<int64_t>(threads, n));
+  for (int w = 0; w < t; ++w)
+    pool.emplace_back([&] {
+      for (;;) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= n) break;
+        body(i);
+      }
+    });
+  for (auto& th : pool) th.join();
+}
+
+extern "C" {
+
+struct gro_policy {
+  double position_rtol, position_atol, momentum_rtol, momentum_atol;
+  double initial_step, minimum_step, maximum_step;
+  double safety, minimum_factor, maximum_factor;
+  uint64_t maximum_accepted_steps;
+  uint32_t maximum_consecutive_rejects;
+  uint32_t policy_id;
+  double event_affine_tolerance, event_tie_tolerance, event_arming_band, singularity_guard;
+};
+
+struct gro_events {
+  int32_t has_escape;
+  int32_t has_surface;
+  double escape_radius;
+  double surface_inner, surface_outer;
+  double horizon_offset;
+  double intensity_at_six;
+};
+
+struct gro_scene {
+  double mass, spin, charge;
+  int32_t chart;  // 0 ingoing, 1 outgoing
+  int32_t pad;
+  double observer_txyz[4];
+  double target_txyz[4];
+  double up_hint[3];
+  double frequency;
+  uint32_t width, height;
+  double vertical_fov;
+};
+
+struct gro_observer_info {
+  double event[4];
+  double g_tt;
+  double gram_residual;
+  double orientation;
+  int32_t used_up_fallback;
+  int32_t extremality;
+  double outer_horizon;  // NaN when absent
+  double four_velocity[4], image_right[4], image_up[4], arrival[4];
+  double metric_covariant[16];
+  double tangent_half_fov;
+};
+
+enum { GRO_FIELDS = 43 };
+
+int gro_fields() { return GRO_FIELDS; }
+
+static Policy to_policy(const gro_policy& p) {
+  Policy q;
+  q.id = int(p.policy_id);
+  q.position_rtol = p.position_rtol;
+  q.position_atol = p.position_atol;
+  q.momentum_rtol = p.momentum_rtol;
+  q.momentum_atol = p.momentum_atol;
+  q.initial_step = p.initial_step;
+  q.minimum_step = p.minimum_step;
+  q.maximum_step = p.maximum_step;
+  q.safety = p.safety;
+  q.minimum_factor = p.minimum_factor;
+  q.maximum_factor = p.maximum_factor;
+  q.maximum_accepted_steps = p.maximum_accepted_steps;
+  q.maximum_consecutive_rejects = p.maximum_consecutive_rejects;
+  q.event_affine_tolerance = p.event_affine_tolerance;
+  q.event_tie_tolerance = p.event_tie_tolerance;
+  q.event_arming_band = p.event_arming_band;
+  q.singularity_guard = p.singularity_guard;
+  return q;
+}
+
+void gro_policy_preset(int which, gro_policy* out) {
+  const Policy p = which == 1 ? Policy::strict_v1() : Policy::regular_v1();
+  *out = {p.position_rtol, p.position_atol, p.momentum_rtol, p.momentum_atol, p.initial_step, p.minimum_step,
+          p.maximum_step, p.safety, p.minimum_factor, p.maximum_factor, p.maximum_accepted_steps,
+          p.maximum_consecutive_rejects, uint32_t(p.id), p.event_affine_tolerance, p.event_tie_tolerance,
+          p.event_arming_band, p.singularity_guard};
+}
+
+static EventConfig to_events(const gro_events& e) {
+  EventConfig c;
+  c.has_escape = e.has_escape != 0;
+  c.escape_radius = e.escape_radius;
+  c.has_surface = e.has_surface != 0;
+  c.surface_inner = e.surface_inner;
+  c.surface_outer = e.surface_outer;
+  c.horizon_offset = e.horizon_offset;
+  return c;
+}
+
+static void pack(const Outcome& o, double* f) {
+  f[0] = double(int(o.termination));
+  f[1] = double(int(o.failure));
+  f[2] = double(o.event_kind);
+  f[3] = double(o.event_candidates);
+  f[4] = o.event_affine;
+  f[5] = o.event_bracket;
+  f[6] = o.event_residual;
+  for (int i = 0; i < 8; ++i) f[7 + i] = o.state[i];
+  f[15] = o.affine_parameter;
+  f[16] = o.has_turning_radius ? 1.0 : 0.0;
+  f[17] = o.turning_radius;
+  f[18] = o.azimuth_advance;
+  f[19] = o.travel_time;
+  f[20] = double(o.polar_side);
+  f[21] = double(o.radial_turnings);
+  f[22] = double(o.equatorial_crossings);
+  f[23] = double(o.azimuth_winding);
+  f[24] = double(o.accepted_steps);
+  f[25] = double(o.rejected_steps);
+  f[26] = double(o.rhs_evaluations);
+  f[27] = o.minimum_step;
+  f[28] = o.maximum_step;
+  f[29] = o.max_null_residual;
+  f[30] = o.max_energy_drift;
+  f[31] = o.max_lz_drift;
+  f[32] = o.max_carter_drift;
+  f[33] = o.has_escape_direction ? 1.0 : 0.0;
+  for (int i = 0; i < 3; ++i) f[34 + i] = o.escape_direction[i];
+  f[37] = double(o.surface_status);
+  f[38] = o.source_radius;
+  f[39] = o.source_azimuth;
+  f[40] = o.frequency_ratio;
+  f[41] = o.emitted_intensity;
+  f[42] = o.observed_intensity;
+}
+
+int gro_hardware_threads() { return int(std::thread::hardware_concurrency()); }
+
+// Spacetime validation + exact horizon (spacetime.rs:134-238). Returns 0 on success.
+int gro_spacetime_info(double m, double a, double q, int chart, int* extremality, double* outer_horizon) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -1;
+  *extremality = int(sp.extremality);
+  double rp;
+  *outer_horizon = sp.outer_horizon_radius(rp) ? rp : std::numeric_limits<double>::quiet_NaN();
+  return 0;
+}
+
+void gro_oblate_to_cartesian(double a, int chart, double r, double polar, double azimuth, double out[3]) {
+  Spacetime sp;
+  sp.spin_m = a;
+  sp.chart = chart ? Chart::Outgoing : Chart::Ingoing;
+  sp.oblate_to_cartesian(r, polar, azimuth, out);
+}
+
+double gro_prograde_isco(double m, double a, double q) { return prograde_isco(m, a, q); }
+
+static int build_scene(const gro_scene& s, Spacetime& sp, StationaryObserver& obs, PerspectiveView& view) {
+  if (!Spacetime::make(s.mass, s.spin, s.charge, s.chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -1;
+  const ObserverError oe = build_observer(sp, s.observer_txyz, s.target_txyz, s.up_hint, s.frequency, obs);
+  if (oe != ObserverError::None) return -10 - int(oe);
+  if (!PerspectiveView::make(s.width, s.height, s.vertical_fov, view)) return -3;
+  return 0;
+}
+
+int gro_observer_info(const gro_scene* s, gro_observer_info* out) {
+  Spacetime sp;
+  StationaryObserver obs;
+  PerspectiveView view;
+  const int rc = build_scene(*s, sp, obs, view);
+  if (rc != 0) return rc;
+  for (int i = 0; i < 4; ++i) {
+    out->event[i] = obs.event[i];
+    out->four_velocity[i] = obs.frame.four_velocity.v[i];
+    out->image_right[i] = obs.frame.image_right.v[i];
+    out->image_up[i] = obs.frame.image_up.v[i];
+    out->arrival[i] = obs.frame.arrival.v[i];
+  }
+  out->g_tt = obs.metric_g_tt;
+  out->gram_residual = obs.frame.gram_residual;
+  out->orientation = obs.frame.orientation_determinant;
+  out->used_up_fallback = obs.frame.used_up_fallback;
+  out->extremality = int(sp.extremality);
+  double rp;
+  out->outer_horizon = sp.outer_horizon_radius(rp) ? rp : std::numeric_limits<double>::quiet_NaN();
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) out->metric_covariant[r * 4 + c] = obs.metric_covariant[r][c];
+  out->tangent_half_fov = view.tangent_half_fov;
+  return 0;
+}
+
+// Initial rays for image samples (scene.rs:211-270). status[i] = 0 on success.
+int gro_initial_rays(const gro_scene* s, int64_t n, const uint32_t* px, const uint32_t* py, const double* sx,
+                     const double* sy, double* states, double* frequency, double* residual, int32_t* status) {
+  Spacetime sp;
+  StationaryObserver obs;
+  PerspectiveView view;
+  const int rc = build_scene(*s, sp, obs, view);
+  if (rc != 0) return rc;
+  for (int64_t i = 0; i < n; ++i) {
+    InitialRay ray;
+    const InitialRayError e = initial_ray(obs, view, px[i], py[i], sx[i], sy[i], ray);
+    status[i] = int(e);
+    if (e == InitialRayError::None) {
+      for (int c = 0; c < 8; ++c) states[8 * i + c] = ray.state[c];
+      frequency[i] = ray.observer_frequency;
+      residual[i] = ray.normalized_null_residual;
+    }
+  }
+  return 0;
+}
+
+// GeodesicTracer::trace over explicit states (geodesic.rs:53-62), ordered batch (batch.rs:31-43).
+int gro_trace_states(double m, double a, double q, int chart, const gro_policy* pol, const gro_events* ev, int64_t n,
+                     const double* states, double direction, int threads, double* out) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -1;
+  if (bits_of(sp.mass_m) != bits_of(1.0)) return -2;  // geodesic.rs:33-35
+  Tracer tr{sp, to_policy(*pol), to_events(*ev)};
+  parallel_for(n, threads, [&](int64_t i) { pack(tr.trace(states + 8 * i, direction), out + GRO_FIELDS * i); });
+  return 0;
+}
+
+// ObservationTracer::trace over image samples (observation.rs:189-231).
+int gro_trace_pixels(const gro_scene* s, const gro_policy* pol, const gro_events* ev, int64_t n, const uint32_t* px,
+                     const uint32_t* py, const double* sx, const double* sy, int threads, double* out,
+                     int32_t* status) {
+  Spacetime sp;
+  StationaryObserver obs;
+  PerspectiveView view;
+  const int rc = build_scene(*s, sp, obs, view);
+  if (rc != 0) return rc;
+  if (bits_of(sp.mass_m) != bits_of(1.0)) return -2;
+  Tracer tr{sp, to_policy(*pol), to_events(*ev)};
+  if (tr.events.has_surface && tr.events.has_escape && tr.events.surface_outer >= tr.events.escape_radius)
+    return -4;  // events.rs:73-78
+  parallel_for(n, threads, [&](int64_t i) {
+    InitialRay ray;
+    const InitialRayError e = initial_ray(obs, view, px[i], py[i], sx[i], sy[i], ray);
+    status[i] = int(e);
+    if (e != InitialRayError::None) return;
+    if (std::fabs(ray.observer_frequency - 1.0) > 32.0 * 2.220446049250313e-16) {
+      status[i] = 100;  // observation.rs:200-202
+      return;
+    }
+    const Outcome o = trace_observation(tr, ray, ev->intensity_at_six);
+    pack(o, out + GRO_FIELDS * i);
+  });
+  return 0;
+}
+
+// surface.rs:12-146 for one terminal state (bolometric vacuum emitter).
+int gro_surface_observable(double m, double a, double q, int chart, double inner, double outer, double intensity,
+                           const double* state, double observer_frequency, double* out5) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
+  Outcome o{};
+  const int s = observable_at(sp, inner, outer, intensity, state, observer_frequency, o);
+  out5[0] = o.source_radius;
+  out5[1] = o.source_azimuth;
+  out5[2] = o.frequency_ratio;
+  out5[3] = o.emitted_intensity;
+  out5[4] = o.observed_intensity;
+  return s;
+}
+
+// Invariants and normalized null residual of one state (spacetime.rs:345-401).
+int gro_invariants(double m, double a, double q, int chart, const double* state, double* out4) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
+  Invariants inv;
+  const GeometryError e = sp.invariants(state, inv);
+  if (e != GeometryError::None) return int(e);
+  out4[0] = inv.energy;
+  out4[1] = inv.angular_momentum_z;
+  out4[2] = inv.carter_constant;
+  out4[3] = inv.normalized_null_residual;
+  return 0;
+}
+
+// Canonical Hamilton right-hand side of one state (spacetime.rs:305-338).
+int gro_hamiltonian_rhs(double m, double a, double q, int chart, const double* state, double* out8) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
+  return int(sp.hamiltonian_rhs(state, out8));
+}
+
+}  // extern "C"
