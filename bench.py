@@ -1,0 +1,381 @@
+"""Benchmark: Mrays/s of the Kerr-Newman null-geodesic trace on a 3840x2160 frame.
+
+Workload (the headline frame of the precision study): Kerr-Newman M = 1, a = 0.9, Q = 0.3,
+outgoing Kerr-Schild chart, static observer at r = 50 M, inclination 75 deg, pinhole 3840x2160,
+30 deg vertical FOV, one ray per pixel centre; escape at r = 1000 M, capture at r_+ + 1e-3,
+Keplerian bolometric surface from the prograde ISCO to 20 M. One step = one frame traced by the
+persistent DP5(4) kernel in MIXED precision (binary32 stepping, binary64 state, shell steps,
+events and renormalisation). Synthetic inputs: the frame is generated on the device from the camera.
+
+`python bench.py [--gpus N --steps K --warmup W] [--impl reference]`
+Prints one JSON line on rank 0. Under torchrun each rank traces its own frame (weak scaling; the
+only collective is the max-reduction of the timings).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT = 3840, 2160
+SPIN, CHARGE, INCL_DEG, R_OBS, FOV_DEG = 0.9, 0.3, 75.0, 50.0, 30.0
+ESCAPE, HORIZON_OFFSET, SURFACE_OUTER = 1000.0, 1e-3, 20.0
+METRIC = "Mrays/s at 3840x2160 a=0.9, mixed vs plain at equal FP64 error; adjoint Mrays/s"
+L2_BYTES = 126 * 2 ** 20
+
+
+def workload_config(precision: str, policy: dict | None = None) -> dict:
+    cfg = {
+        "workload": f"kerr-newman-frame-{WIDTH}x{HEIGHT}", "width": WIDTH, "height": HEIGHT, "spin": SPIN,
+        "charge": CHARGE, "inclination_deg": INCL_DEG, "observer_radius_m": R_OBS, "vertical_fov_deg": FOV_DEG,
+        "escape_radius_m": ESCAPE, "capture": "r_+ + 1e-3", "surface": "prograde ISCO .. 20 M", "chart": "outgoing",
+        "precision": precision, "stepper": "DP5(4) adaptive",
+        "l2": "L2 flushed between timed frames (256 MiB write); results 1.46 GB/frame exceed L2",
+    }
+    if policy:
+        cfg["policy"] = policy
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def fp32_fma_peak_tflops(sm_count: int, sm_mhz: float) -> float:
+    # 128 FP32 lanes per SM, one FMA (2 flops) per lane per clock
+    return sm_count * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def make_observation(G, width=WIDTH, height=HEIGHT):
+    isco = G.prograde_isco(SPIN, CHARGE)
+    return G.Observation.from_oblate(R_OBS, math.radians(INCL_DEG), 0.0, spin=SPIN, charge=CHARGE,
+                                     chart=G.KerrSchildChart.OUTGOING, width=width, height=height,
+                                     vertical_fov=math.radians(FOV_DEG), escape_radius=ESCAPE,
+                                     surface=G.EquatorialSurface(isco, SURFACE_OUTER), horizon_offset=HORIZON_OFFSET)
+
+
+def sample_pixels(n: int, seed: int = 64):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(WIDTH * HEIGHT, size=n, replace=False))
+    return idx % WIDTH, idx // WIDTH, idx
+
+
+def cpu_oracle_sample(G, n_rays: int, threads: int):
+    """Binary64 oracle (rtol 1e-10, atol 1e-12) on a seeded pixel sample of the frame."""
+    import oracle as O
+
+    obs = make_observation(G)
+    osc = O.scene(mass=1.0, spin=SPIN, charge=CHARGE, chart=1, observer_txyz=obs.observer_txyz, width=WIDTH,
+                  height=HEIGHT, vertical_fov=obs.vertical_fov)
+    ev = O.events(escape_radius=ESCAPE, surface=(obs.surface.inner_radius, SURFACE_OUTER),
+                  horizon_offset=HORIZON_OFFSET)
+    px, py, idx = sample_pixels(n_rays)
+    t0 = time.perf_counter()
+    ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
+    dt = time.perf_counter() - t0
+    return ref, idx, dt
+
+
+def run_reference(args) -> None:
+    """The reference's CPU algorithm (binary64 oracle port) on the host cores, bounded samples."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import gravlume_b200 as G
+    import oracle as O
+
+    threads = O.hardware_threads()
+    n = args.cpu_sample
+    times = []
+    for _ in range(args.warmup):
+        cpu_oracle_sample(G, max(n // 8, 64), threads)
+    for _ in range(args.steps):
+        _, _, dt = cpu_oracle_sample(G, n, threads)
+        times.append(dt)
+    total = sum(times)
+    value = n * len(times) / total / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config("f64 (CPU oracle, rtol 1e-10)"),
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} seeded pixels of the {WIDTH}x{HEIGHT} frame per step"},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def error_report(G, gpu: dict, ref, idx) -> dict:
+    import numpy as np
+    import oracle as O
+
+    F = O.F
+    sel = idx
+    gt = gpu["termination"][sel]
+    ot = ref[:, F["termination"]].astype(int)
+    same = gt == ot
+    rep = {"rays": int(sel.size), "class_mismatch": int((~same).sum())}
+    esc = same & (ot == 2)
+    if esc.any():
+        d = np.stack([ref[esc, F["escape_dx"]], ref[esc, F["escape_dy"]], ref[esc, F["escape_dz"]]], axis=1)
+        th, ph = gpu["escape_theta"][sel][esc], gpu["escape_phi"][sel][esc]
+        v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+        rep["escape_direction_rad"] = float(np.max(np.arccos(np.clip((d * v).sum(1), -1, 1))))
+    srf = same & (ot == 7)
+    if srf.any():
+        g0 = ref[srf, F["frequency_ratio"]]
+        rep["g_rel"] = float(np.max(np.abs(gpu["frequency_ratio"][sel][srf] - g0) / g0))
+        rep["hit_radius"] = float(np.max(np.abs(gpu["source_radius"][sel][srf] - ref[srf, F["source_radius"]])))
+    if same.any():
+        rep["travel_time"] = float(np.max(np.abs(gpu["travel_time"][sel][same] - ref[same, F["travel_time"]])))
+        for k in ("max_null_residual", "max_lz_drift", "max_carter_drift"):
+            rep[k] = float(np.max(np.abs(gpu[k][sel][same] - ref[same, F[k]])))
+        rep["event_residual_max"] = float(np.nanmax(gpu["event_residual"][sel][same]))
+    return rep
+
+
+def run_gpu(args) -> None:
+    import numpy as np
+    import torch
+
+    import gravlume_b200 as G
+    from gravlume_b200 import _native as N
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    obs = make_observation(G)
+    scene = obs.pack()
+    cam = G.image_camera(0, WIDTH, HEIGHT)
+    pipe = G.TracePipeline(local)
+    precision = {"fp32": G.Precision.FP32, "mixed": G.Precision.MIXED, "fp64": G.Precision.FP64}[args.precision]
+    pipe.set_policy(G.ReferencePolicy.frame(precision))
+    results = G.TraceResults(WIDTH * HEIGHT, dev)
+    stream = torch.cuda.current_stream()
+    if args.autotune:
+        small = make_observation(G, WIDTH // 4, HEIGHT // 4)
+        pipe.autotune([small.pack()], [G.image_camera(0, WIDTH // 4, HEIGHT // 4)], repeats=1)
+    policy = pipe.policy.as_dict()
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        pipe.trace([scene], [cam], results, stream=stream)
+    torch.cuda.synchronize()
+    launches0 = pipe.stats().kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            ev[k][0].record(stream)
+            pipe.trace([scene], [cam], results, stream=stream)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    launches = pipe.stats().kernel_launches - launches0
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    rays = WIDTH * HEIGHT
+    value = world * rays * args.steps / (total_ms / 1e3) / 1e6
+    d = results.numpy()
+
+    # ---- end to end through the host-buffer call (H2D job table, trace, D2H of every field)
+    e2e_ms = None
+    host = G.TraceResults(WIDTH * HEIGHT, None, host=True)
+    e2e_steps = max(1, min(args.steps, 2))
+    pipe.trace_host([scene], [cam])  # warm the workspace
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sa, ca = pipe._arrays([scene], [cam])
+        rs = host.struct()
+        N.check(N.lib().glc_trace_host(pipe._h, sa, 1, ca, 1, rs), "glc_trace_host")
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+           "h2d_bytes_per_step": int(ctypes_sizeof_job()), "d2h_bytes_per_step": int(WIDTH * HEIGHT * 16 * 11)}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline: algorithmic flops of the attempted steps / average launch duration
+    flops = np.zeros(4)
+    N.lib().glc_flop_model(flops.ctypes.data)
+    attempts = float(d["accepted_steps"].sum() + d["rejected_steps"].sum())
+    alg_flops = attempts * flops[2]
+    launch_s = (total_ms / args.steps) / 1e3
+    achieved_tflops = alg_flops / launch_s / 1e12
+    clk = clocks.summary()
+    sm_count = pipe.stats().sm_count
+    peak_mhz = clk["sm_mhz"] or 1965.0
+    peak = fp32_fma_peak_tflops(sm_count, peak_mhz)
+    roofline = {"bound": "fp32_fma", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved_tflops / peak,
+                "peak_source": f"nominal {sm_count} SMs x 128 FP32 lanes x 2 x median SM clock {peak_mhz:.0f} MHz "
+                               "under load (MEASURED_PEAKS.json has no FP32 figure)",
+                "alg_flops_per_launch": alg_flops, "attempted_steps": attempts,
+                "flops_per_attempt": float(flops[2]), "traffic": args.traffic_bytes}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp32": "f32", "mixed": "f32+f64", "fp64": "f64"}[args.precision],
+        "data": "synthetic (camera rays generated on device)", "config": workload_config(args.precision, policy),
+        "gpu_launches": int(launches), "clocks": clk, "e2e": e2e, "roofline": roofline,
+        "class_histogram": np.bincount(d["termination"], minlength=9).tolist(),
+        "steps_per_ray": {"mean": float(d["accepted_steps"].mean()), "max": int(d["accepted_steps"].max()),
+                          "rejected_mean": float(d["rejected_steps"].mean())},
+    }
+
+    # ---- precision study on the same frame: plain FP32 and FP64 at the same job, errors vs the oracle
+    if args.compare:
+        comp = {}
+        ref = idx = None
+        if args.cpu_sample > 0:
+            import oracle as O
+
+            threads = O.hardware_threads()
+            ref, idx, cpu_s = cpu_oracle_sample(G, args.cpu_sample, threads)
+            line["cpu_baseline"] = {"value": args.cpu_sample / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
+                                    "kind": "port",
+                                    "sample": f"{args.cpu_sample} seeded pixels of the {WIDTH}x{HEIGHT} frame, "
+                                              "binary64 oracle rtol 1e-10 atol 1e-12"}
+            comp[args.precision] = error_report(G, d, ref, idx)
+        for name, prec in (("fp32", G.Precision.FP32), ("fp64", G.Precision.FP64)):
+            if name == args.precision:
+                continue
+            pipe.set_policy(G.ReferencePolicy.frame(prec, **{k: policy[k] for k in (
+                "persistent", "block_threads", "tile_w", "tile_h", "refill_interval", "rays_per_grab")}))
+            pipe.trace([scene], [cam], results, stream=stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            pipe.trace([scene], [cam], results, stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            dd = results.numpy()
+            entry = {"mrays_per_s": rays / (ms / 1e3) / 1e6, "ms": ms}
+            if ref is not None:
+                entry["error_vs_oracle"] = error_report(G, dd, ref, idx)
+            comp[name] = entry
+        comp[args.precision] = {"mrays_per_s": value / world, "ms": total_ms / args.steps,
+                                "error_vs_oracle": comp.get(args.precision)}
+        line["precision_study"] = comp
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def ctypes_sizeof_job() -> int:
+    from gravlume_b200 import _native as N
+    import ctypes
+
+    return ctypes.sizeof(N.Scene) + ctypes.sizeof(N.Camera) + 16
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-compare", dest="compare", action="store_false")
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=2048,
+                    help="pixels of the frame traced by the CPU oracle (baseline and error report)")
+    ap.add_argument("--traffic-bytes", type=float, default=None,
+                    help="DRAM bytes per launch from an ncu capture, reported as roofline.traffic")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

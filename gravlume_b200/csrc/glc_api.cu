@@ -1,0 +1,651 @@
+// C ABI implementation: contexts, job tables, trace launches, CUDA graphs and the autotuner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "glc_internal.h"
+#include "glc_kernels.cuh"
+
+using namespace glc;
+
+namespace glc {
+namespace {
+thread_local std::string g_last_error;
+}
+
+glc_status set_error(glc_status status, const char* message) {
+  g_last_error = message ? message : "";
+  return status;
+}
+}  // namespace glc
+
+#define GLC_CUDA(expr)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      std::string m_ = std::string(#expr) + ": " + cudaGetErrorString(e_);                      \
+      return set_error(GLC_ERR_CUDA, m_.c_str());                                               \
+    }                                                                                           \
+  } while (0)
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Host-side description of a job: padded ray counts per camera and the device-table layout.
+struct JobLayout {
+  std::vector<unsigned long long> begin;
+  unsigned long long total = 0;
+  size_t off_scenes = 0, off_cams = 0, off_begin = 0, bytes = 0;
+};
+
+glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cams, int32_t n_cams,
+                        const glc_policy& pol, JobLayout& L) {
+  if (!scenes || !cams || n_scenes <= 0 || n_cams <= 0)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "scenes and cameras must be non-empty");
+  if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
+  L.begin.assign(size_t(n_cams) + 1, 0);
+  unsigned long long acc = 0;
+  for (int i = 0; i < n_cams; ++i) {
+    const glc_camera& c = cams[i];
+    if (c.scene_index < 0 || c.scene_index >= n_scenes)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "camera scene index out of range");
+    unsigned long long n = 0;
+    if (c.kind == GLC_CAMERA_RAYLIST) {
+      if (!c.ray_states && c.n_rays > 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "ray list needs states");
+      if (!(c.affine_direction == 1.0 || c.affine_direction == -1.0))
+        return set_error(GLC_ERR_INVALID_ARGUMENT, "affine direction must be +1 or -1");
+      if ((reinterpret_cast<uintptr_t>(c.ray_states) & 15u) != 0)
+        return set_error(GLC_ERR_INVALID_ARGUMENT, "ray states must be 16-byte aligned");
+      n = c.n_rays;
+    } else if (c.kind == GLC_CAMERA_PINHOLE || c.kind == GLC_CAMERA_EQUIRECT) {
+      if (c.width == 0 || c.height == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera size must be nonzero");
+      if (!(c.subpixel_x >= 0.0 && c.subpixel_x <= 1.0 && c.subpixel_y >= 0.0 && c.subpixel_y <= 1.0))
+        return set_error(GLC_ERR_INVALID_ARGUMENT, "subpixel offsets must lie in [0, 1]");
+      if (c.kind == GLC_CAMERA_PINHOLE &&
+          (c.width != scenes[c.scene_index].width || c.height != scenes[c.scene_index].height))
+        return set_error(GLC_ERR_INVALID_ARGUMENT, "pinhole camera size must match the scene's view");
+      const unsigned long long tx = (c.width + pol.tile_w - 1) / pol.tile_w;
+      const unsigned long long ty = (c.height + pol.tile_h - 1) / pol.tile_h;
+      n = tx * ty * pol.tile_w * pol.tile_h;
+    } else {
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown camera kind");
+    }
+    L.begin[i] = acc;
+    acc += n;
+  }
+  L.begin[n_cams] = acc;
+  L.total = acc;
+  L.off_scenes = 0;
+  L.off_cams = align256(sizeof(glc_scene) * n_scenes);
+  L.off_begin = L.off_cams + align256(sizeof(glc_camera) * n_cams);
+  L.bytes = L.off_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
+  return GLC_OK;
+}
+
+void fill_staging(unsigned char* stage, const JobLayout& L, const glc_scene* scenes, int32_t n_scenes,
+                  const glc_camera* cams, int32_t n_cams) {
+  std::memcpy(stage + L.off_scenes, scenes, sizeof(glc_scene) * n_scenes);
+  std::memcpy(stage + L.off_cams, cams, sizeof(glc_camera) * n_cams);
+  std::memcpy(stage + L.off_begin, L.begin.data(), sizeof(unsigned long long) * (n_cams + 1));
+}
+
+JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
+  JobView v;
+  v.scenes = reinterpret_cast<const glc_scene*>(dev + L.off_scenes);
+  v.cams = reinterpret_cast<const glc_camera*>(dev + L.off_cams);
+  v.begin = reinterpret_cast<const unsigned long long*>(dev + L.off_begin);
+  v.n_cams = n_cams;
+  v.total = L.total;
+  return v;
+}
+
+}  // namespace
+
+struct glc_ctx {
+  int device = 0;
+  int sm_count = 0;
+  glc_policy policy{};
+  unsigned char* d_job = nullptr;
+  size_t d_job_bytes = 0;
+  unsigned char* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+  cudaEvent_t stage_free = nullptr;  // recorded after the last staging copy
+  bool stage_pending = false;
+  unsigned long long* d_queue = nullptr;
+  unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
+  size_t d_host_ws_bytes = 0;
+  glc_launch_stats stats{};
+};
+
+struct glc_graph {
+  glc_ctx* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned char* d_job = nullptr;
+  unsigned char* h_stage = nullptr;
+  unsigned long long* d_queue = nullptr;
+};
+
+namespace {
+
+template <int P>
+glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out,
+                            cudaStream_t stream, unsigned long long* queue) {
+  const unsigned block = pol.block_threads;
+  if (pol.persistent) {
+    int per_sm = int(pol.blocks_per_sm);
+    if (per_sm <= 0) {
+      GLC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<P>, int(block), 0));
+      if (per_sm <= 0) per_sm = 1;
+    }
+    const unsigned long long warps_needed = (job.total + 31) / 32;
+    unsigned long long grid = (unsigned long long)ctx->sm_count * per_sm;
+    const unsigned long long grid_cap = (warps_needed * 32 + block - 1) / block;
+    if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
+    GLC_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream));
+    trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+    ctx->stats.last_grid = unsigned(grid);
+    ctx->stats.kernel_launches += 1;
+  } else {
+    const unsigned long long grid = (job.total + block - 1) / block;
+    if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
+    trace_simple_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out);
+    ctx->stats.last_grid = unsigned(grid);
+    ctx->stats.kernel_launches += 1;
+  }
+  GLC_CUDA(cudaGetLastError());
+  ctx->stats.last_block = block;
+  ctx->stats.last_persistent = pol.persistent;
+  ctx->stats.last_rays = job.total;
+  return GLC_OK;
+}
+
+glc_status launch(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out, cudaStream_t stream,
+                  unsigned long long* queue) {
+  if (job.total == 0) return GLC_OK;
+  if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
+  switch (pol.precision) {
+    case GLC_FP32: return launch_precision<kFP32>(ctx, job, pol, out, stream, queue);
+    case GLC_MIXED: return launch_precision<kMIXED>(ctx, job, pol, out, stream, queue);
+    case GLC_FP64: return launch_precision<kFP64>(ctx, job, pol, out, stream, queue);
+    default: return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown precision mode");
+  }
+}
+
+glc_status validate_policy(const glc_policy& p) {
+  const double v[] = {p.position_rtol, p.position_atol, p.momentum_rtol, p.momentum_atol, p.initial_step,
+                      p.minimum_step,  p.maximum_step,  p.safety,        p.minimum_factor, p.maximum_factor};
+  for (double x : v)
+    if (!std::isfinite(x) || x <= 0.0) return set_error(GLC_ERR_INVALID_ARGUMENT, "policy values must be positive");
+  if (p.minimum_step > p.maximum_step) return set_error(GLC_ERR_INVALID_ARGUMENT, "minimum step exceeds maximum step");
+  if (p.maximum_consecutive_rejects == 0 || p.maximum_accepted_steps == 0)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "step and reject limits must be positive");
+  if (p.precision < GLC_FP32 || p.precision > GLC_FP64) return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!(p.event_affine_tolerance > 0.0) || !(p.event_tie_tolerance >= 0.0) || !(p.event_arming_band >= 0.0) ||
+      !(p.singularity_guard > 0.0))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "event tolerances must be positive");
+  if (p.block_threads == 0 || p.block_threads % 32 != 0 || p.block_threads > 128)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
+  if (p.tile_w == 0 || p.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
+  return GLC_OK;
+}
+
+glc_status ensure_job_capacity(glc_ctx* ctx, size_t bytes) {
+  if (ctx->stage_pending) {
+    GLC_CUDA(cudaEventSynchronize(ctx->stage_free));
+    ctx->stage_pending = false;
+  }
+  if (bytes > ctx->d_job_bytes) {
+    if (ctx->d_job) GLC_CUDA(cudaFree(ctx->d_job));
+    ctx->d_job = nullptr;
+    GLC_CUDA(cudaMalloc(&ctx->d_job, bytes));
+    ctx->d_job_bytes = bytes;
+  }
+  if (bytes > ctx->h_stage_bytes) {
+    if (ctx->h_stage) GLC_CUDA(cudaFreeHost(ctx->h_stage));
+    ctx->h_stage = nullptr;
+    GLC_CUDA(cudaMallocHost(&ctx->h_stage, bytes));
+    ctx->h_stage_bytes = bytes;
+  }
+  return GLC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int glc_abi_version(void) { return GLC_ABI_VERSION; }
+
+const char* glc_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* glc_status_string(glc_status s) {
+  switch (s) {
+    case GLC_OK: return "ok";
+    case GLC_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case GLC_ERR_CUDA: return "CUDA error";
+    case GLC_ERR_NON_FINITE: return "non-finite input";
+    case GLC_ERR_NON_POSITIVE: return "non-positive input";
+    case GLC_ERR_NON_NORMALIZED: return "observer frequency not normalized";
+    case GLC_ERR_EXTREMALITY_CHANGED: return "extremality changed by normalization";
+    case GLC_ERR_NON_STATIONARY: return "observer is not stationary";
+    case GLC_ERR_DEGENERATE_FRAME: return "degenerate observer frame";
+    case GLC_ERR_SURFACE_OUTSIDE_ESCAPE: return "surface outside the escape sphere";
+    case GLC_ERR_INVALID_SURFACE: return "invalid surface";
+    case GLC_ERR_INVALID_VIEW: return "invalid view";
+    case GLC_ERR_TIMEOUT: return "device wait timed out";
+    case GLC_ERR_CAPACITY: return "capacity exceeded";
+    case GLC_ERR_NO_DEVICE: return "no CUDA device";
+    case GLC_ERR_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+glc_status glc_scene_pack(const glc_scene_input* input, glc_scene* out) {
+  if (!input || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  return pack_scene(*input, *out);
+}
+
+glc_status glc_prograde_isco(double spin, double charge, double* out) {
+  if (!out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (!std::isfinite(spin) || !std::isfinite(charge)) return set_error(GLC_ERR_NON_FINITE, "non-finite input");
+  if (spin * spin + charge * charge >= 1.0) return set_error(GLC_ERR_INVALID_ARGUMENT, "ISCO needs a subextremal hole");
+  *out = prograde_isco(spin, charge);
+  return GLC_OK;
+}
+
+glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out) {
+  if (!out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (precision < GLC_FP32 || precision > GLC_FP64) return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown precision");
+  glc_policy p{};
+  // reference-regular-v1 (crates/gravlume-reference/src/policy.rs:28-48)
+  p.position_rtol = p.momentum_rtol = 2.0e-12;
+  p.position_atol = p.momentum_atol = 2.0e-13;
+  p.initial_step = 1.0e-3;
+  p.minimum_step = 9.094947017729282e-13;
+  p.maximum_step = 0.5;
+  p.safety = 0.9;
+  p.minimum_factor = 0.2;
+  p.maximum_factor = 5.0;
+  p.maximum_accepted_steps = 200000;
+  p.maximum_consecutive_rejects = 64;
+  p.event_affine_tolerance = 2.0e-11;
+  p.event_tie_tolerance = 5.0e-11;
+  p.event_arming_band = 1.28e-9;
+  p.singularity_guard = 9.094947017729282e-13;
+  if (preset == 1) {  // reference-strict-v1 (policy.rs:51-66)
+    p.position_rtol /= 16.0;
+    p.momentum_rtol /= 16.0;
+    p.position_atol /= 16.0;
+    p.momentum_atol /= 16.0;
+    p.maximum_step = 0.25;
+    p.maximum_accepted_steps *= 2;
+    p.maximum_consecutive_rejects *= 2;
+    p.event_affine_tolerance /= 4.0;
+    p.event_tie_tolerance /= 4.0;
+  } else if (preset == 2) {
+    // frame policy: binary64 modes at rtol 1e-10 / atol 1e-12; binary32 stepping at a tolerance
+    // its arithmetic can honour, with event tolerances scaled to its resolution
+    if (precision == GLC_FP64) {
+      p.position_rtol = p.momentum_rtol = 1.0e-10;
+      p.position_atol = p.momentum_atol = 1.0e-12;
+    } else {
+      p.position_rtol = p.momentum_rtol = 1.0e-6;
+      p.position_atol = p.momentum_atol = 1.0e-8;
+      if (precision == GLC_FP32) {
+        p.event_affine_tolerance = 1.0e-6;
+        p.event_tie_tolerance = 2.0e-6;
+        p.event_arming_band = 1.0e-5;
+      }
+    }
+  } else if (preset != 0) {
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown policy preset");
+  }
+  p.precision = precision;
+  p.mixed_shell_factor = 1.2;
+  p.renormalize_null = precision == GLC_MIXED ? 1u : 0u;
+  p.persistent = 1;
+  p.block_threads = 128;
+  p.blocks_per_sm = 0;
+  p.tile_w = 8;
+  p.tile_h = 4;
+  p.refill_interval = 8;
+  p.rays_per_grab = 64;
+  *out = p;
+  return GLC_OK;
+}
+
+glc_status glc_flop_model(double out4[4]) {
+  if (!out4) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  flop_model(out4);
+  return GLC_OK;
+}
+
+glc_status glc_rhs_host(const glc_scene* scene, const double state6[6], double energy, int32_t precision,
+                        double out7[7]) {
+  if (!scene || !state6 || !out7) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  const LaneScene ls = make_lane_scene(*scene, 1.0);
+  if (precision == GLC_FP32) {
+    const KN<float> k = kn_cast<float>(ls.kn);
+    float y[6], d[7], r, vr;
+    for (int i = 0; i < 6; ++i) y[i] = float(state6[i]);
+    kn_rhs(k, y, float(energy), d, r, vr);
+    for (int i = 0; i < 7; ++i) out7[i] = d[i];
+  } else {
+    double r, vr;
+    kn_rhs(ls.kn, state6, energy, out7, r, vr);
+  }
+  return GLC_OK;
+}
+
+glc_status glc_create(int32_t device, glc_ctx** out) {
+  if (!out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return set_error(GLC_ERR_NO_DEVICE, "no CUDA device is available");
+  }
+  if (device < 0 || device >= count) return set_error(GLC_ERR_INVALID_ARGUMENT, "device index out of range");
+  DeviceGuard g(device);
+  glc_ctx* ctx = new glc_ctx();
+  ctx->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    delete ctx;
+    return set_error(GLC_ERR_CUDA, "cudaGetDeviceProperties failed");
+  }
+  ctx->sm_count = prop.multiProcessorCount;
+  ctx->stats.sm_count = unsigned(prop.multiProcessorCount);
+  glc_policy_default(2, GLC_MIXED, &ctx->policy);
+  if (cudaMalloc(&ctx->d_queue, 256) != cudaSuccess || cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming) != cudaSuccess) {
+    if (ctx->d_queue) cudaFree(ctx->d_queue);
+    delete ctx;
+    return set_error(GLC_ERR_CUDA, "context allocation failed");
+  }
+  *out = ctx;
+  return GLC_OK;
+}
+
+glc_status glc_destroy(glc_ctx* ctx) {
+  if (!ctx) return GLC_OK;
+  DeviceGuard g(ctx->device);
+  if (ctx->stage_pending) cudaEventSynchronize(ctx->stage_free);
+  if (ctx->d_job) cudaFree(ctx->d_job);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+  if (ctx->d_queue) cudaFree(ctx->d_queue);
+  if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
+  if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
+  delete ctx;
+  return GLC_OK;
+}
+
+glc_status glc_set_policy(glc_ctx* ctx, const glc_policy* policy) {
+  if (!ctx || !policy) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  const glc_status s = validate_policy(*policy);
+  if (s != GLC_OK) return s;
+  ctx->policy = *policy;
+  return GLC_OK;
+}
+
+glc_status glc_get_policy(const glc_ctx* ctx, glc_policy* out) {
+  if (!ctx || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  *out = ctx->policy;
+  return GLC_OK;
+}
+
+glc_status glc_get_stats(const glc_ctx* ctx, glc_launch_stats* out) {
+  if (!ctx || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  *out = ctx->stats;
+  return GLC_OK;
+}
+
+glc_status glc_result_slots(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras, int32_t n_cameras,
+                            uint64_t* out) {
+  if (!out || !cameras || n_cameras <= 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  uint64_t m = 0;
+  for (int i = 0; i < n_cameras; ++i) {
+    const glc_camera& c = cameras[i];
+    uint64_t n = c.kind == GLC_CAMERA_RAYLIST ? c.n_rays : uint64_t(c.width) * c.height;
+    m = std::max<uint64_t>(m, c.result_offset + n);
+  }
+  (void)scenes;
+  (void)n_scenes;
+  *out = m;
+  return GLC_OK;
+}
+
+glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                     int32_t n_cameras, const glc_results* out, void* stream) {
+  if (!ctx || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(ctx->device);
+  JobLayout L;
+  glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
+  if (s != GLC_OK) return s;
+  s = ensure_job_capacity(ctx, L.bytes);
+  if (s != GLC_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  fill_staging(ctx->h_stage, L, scenes, n_scenes, cameras, n_cameras);
+  GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, st));
+  GLC_CUDA(cudaEventRecord(ctx->stage_free, st));
+  ctx->stage_pending = true;
+  return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue);
+}
+
+glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                          int32_t n_cameras, const glc_results* host_out) {
+  if (!ctx || !host_out || !cameras || n_cameras <= 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(ctx->device);
+  uint64_t slots = 0;
+  glc_status s = glc_result_slots(scenes, n_scenes, cameras, n_cameras, &slots);
+  if (s != GLC_OK) return s;
+  void* hfields[11] = {host_out->code,    host_out->branch,  host_out->escape,      host_out->surface,
+                       host_out->redshift_time, host_out->event, host_out->drift_a, host_out->drift_b,
+                       host_out->turning, host_out->position_xy, host_out->position_zr};
+  // workspace layout: ray-list states, then one 16-byte-per-slot array per requested field
+  std::vector<size_t> state_off(size_t(n_cameras), 0);
+  size_t bytes = 0;
+  for (int i = 0; i < n_cameras; ++i)
+    if (cameras[i].kind == GLC_CAMERA_RAYLIST && cameras[i].n_rays > 0) {
+      state_off[i] = bytes;
+      bytes += align256(cameras[i].n_rays * 8 * sizeof(double));
+    }
+  size_t field_off[11];
+  for (int i = 0; i < 11; ++i) {
+    field_off[i] = bytes;
+    if (hfields[i]) bytes += align256(slots * 16);
+  }
+  if (bytes > ctx->d_host_ws_bytes) {
+    if (ctx->d_host_ws) GLC_CUDA(cudaFree(ctx->d_host_ws));
+    ctx->d_host_ws = nullptr;
+    ctx->d_host_ws_bytes = 0;
+    GLC_CUDA(cudaMalloc(&ctx->d_host_ws, bytes));
+    ctx->d_host_ws_bytes = bytes;
+  }
+  std::vector<glc_camera> cams(cameras, cameras + n_cameras);
+  for (int i = 0; i < n_cameras; ++i) {
+    if (cams[i].kind == GLC_CAMERA_RAYLIST && cams[i].n_rays > 0) {
+      unsigned char* d = ctx->d_host_ws + state_off[i];
+      GLC_CUDA(cudaMemcpyAsync(d, cameras[i].ray_states, cams[i].n_rays * 8 * sizeof(double), cudaMemcpyHostToDevice,
+                               nullptr));
+      cams[i].ray_states = reinterpret_cast<const double*>(d);
+    }
+  }
+  glc_results dev{};
+  void** dfields[11] = {(void**)&dev.code,    (void**)&dev.branch,  (void**)&dev.escape,      (void**)&dev.surface,
+                        (void**)&dev.redshift_time, (void**)&dev.event, (void**)&dev.drift_a, (void**)&dev.drift_b,
+                        (void**)&dev.turning, (void**)&dev.position_xy, (void**)&dev.position_zr};
+  for (int i = 0; i < 11; ++i) *dfields[i] = hfields[i] ? ctx->d_host_ws + field_off[i] : nullptr;
+  s = glc_trace(ctx, scenes, n_scenes, cams.data(), n_cameras, &dev, nullptr);
+  if (s != GLC_OK) return s;
+  for (int i = 0; i < 11; ++i) {
+    if (!hfields[i]) continue;
+    GLC_CUDA(cudaMemcpyAsync(hfields[i], *dfields[i], slots * 16, cudaMemcpyDeviceToHost, nullptr));
+  }
+  GLC_CUDA(cudaStreamSynchronize(nullptr));
+  return GLC_OK;
+}
+
+glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                             int32_t n_cameras, const glc_results* out, void* stream, glc_graph** graph) {
+  if (!ctx || !out || !graph) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (!stream) return set_error(GLC_ERR_INVALID_ARGUMENT, "graph capture needs a non-default stream");
+  *graph = nullptr;
+  DeviceGuard g(ctx->device);
+  JobLayout L;
+  glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
+  if (s != GLC_OK) return s;
+  glc_graph* G = new glc_graph();
+  G->ctx = ctx;
+  auto fail = [&](glc_status st) {
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    if (G->d_job) cudaFree(G->d_job);
+    if (G->h_stage) cudaFreeHost(G->h_stage);
+    if (G->d_queue) cudaFree(G->d_queue);
+    delete G;
+    return st;
+  };
+  if (cudaMalloc(&G->d_job, L.bytes) != cudaSuccess || cudaMallocHost(&G->h_stage, L.bytes) != cudaSuccess ||
+      cudaMalloc(&G->d_queue, 256) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "graph buffer allocation failed"));
+  fill_staging(G->h_stage, L, scenes, n_scenes, cameras, n_cameras);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "cudaStreamBeginCapture failed"));
+  cudaError_t ce = cudaMemcpyAsync(G->d_job, G->h_stage, L.bytes, cudaMemcpyHostToDevice, st);
+  glc_status ls = ce == cudaSuccess ? launch(ctx, job_view(G->d_job, L, n_cameras), ctx->policy, *out, st, G->d_queue)
+                                    : set_error(GLC_ERR_CUDA, cudaGetErrorString(ce));
+  cudaGraph_t gr = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(st, &gr);
+  if (ls != GLC_OK) {
+    if (gr) cudaGraphDestroy(gr);
+    return fail(ls);
+  }
+  if (ee != cudaSuccess) return fail(set_error(GLC_ERR_CUDA, cudaGetErrorString(ee)));
+  G->graph = gr;
+  if (cudaGraphInstantiate(&G->exec, gr, 0) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "cudaGraphInstantiate failed"));
+  *graph = G;
+  return GLC_OK;
+}
+
+glc_status glc_graph_launch(glc_graph* graph, void* stream) {
+  if (!graph) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(graph->ctx->device);
+  GLC_CUDA(cudaGraphLaunch(graph->exec, static_cast<cudaStream_t>(stream)));
+  graph->ctx->stats.kernel_launches += 1;
+  return GLC_OK;
+}
+
+glc_status glc_graph_destroy(glc_graph* graph) {
+  if (!graph) return GLC_OK;
+  DeviceGuard g(graph->ctx->device);
+  cudaDeviceSynchronize();
+  if (graph->exec) cudaGraphExecDestroy(graph->exec);
+  if (graph->graph) cudaGraphDestroy(graph->graph);
+  if (graph->d_job) cudaFree(graph->d_job);
+  if (graph->h_stage) cudaFreeHost(graph->h_stage);
+  if (graph->d_queue) cudaFree(graph->d_queue);
+  delete graph;
+  return GLC_OK;
+}
+
+glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                        int32_t n_cameras, const glc_results* out, void* stream, int32_t repeats, glc_policy* policy) {
+  if (!ctx || !out || !policy) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(ctx->device);
+  if (repeats < 1) repeats = 1;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t e0, e1;
+  GLC_CUDA(cudaEventCreate(&e0));
+  GLC_CUDA(cudaEventCreate(&e1));
+  const glc_policy saved = ctx->policy;
+  glc_policy best = *policy;
+  float best_ms = std::numeric_limits<float>::infinity();
+  auto time_policy = [&](const glc_policy& cand, float& ms) -> glc_status {
+    glc_status s = validate_policy(cand);
+    if (s != GLC_OK) return s;
+    ctx->policy = cand;
+    s = glc_trace(ctx, scenes, n_scenes, cameras, n_cameras, out, stream);  // warm-up
+    if (s != GLC_OK) return s;
+    GLC_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < repeats; ++r) {
+      s = glc_trace(ctx, scenes, n_scenes, cameras, n_cameras, out, stream);
+      if (s != GLC_OK) return s;
+    }
+    GLC_CUDA(cudaEventRecord(e1, st));
+    GLC_CUDA(cudaEventSynchronize(e1));
+    GLC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= float(repeats);
+    return GLC_OK;
+  };
+  // coordinate descent over the launch-shape knobs, starting from the caller's policy
+  struct Knob {
+    int which;
+    std::vector<uint32_t> values;
+  };
+  const std::vector<std::pair<uint32_t, uint32_t>> tiles = {{8, 4}, {16, 2}, {32, 1}, {4, 8}, {8, 8}, {16, 16}};
+  const std::vector<Knob> knobs = {
+      {0, {0, 1}},             // persistent
+      {1, {64, 96, 128}},      // block threads
+      {2, {0, 1, 2, 3, 4, 5}}, // tile index
+      {3, {32, 64, 128, 256}}, // rays per grab
+      {4, {1, 4, 8, 16, 32}},  // refill interval
+  };
+  glc_status s = time_policy(best, best_ms);
+  for (int pass = 0; pass < 2 && s == GLC_OK; ++pass) {
+    for (const Knob& k : knobs) {
+      for (uint32_t v : k.values) {
+        glc_policy cand = best;
+        switch (k.which) {
+          case 0: cand.persistent = v; break;
+          case 1: cand.block_threads = v; break;
+          case 2: cand.tile_w = tiles[v].first; cand.tile_h = tiles[v].second; break;
+          case 3: cand.rays_per_grab = v; break;
+          case 4: cand.refill_interval = v; break;
+        }
+        if (!cand.persistent && (k.which == 3 || k.which == 4)) continue;
+        float ms = 0.0f;
+        s = time_policy(cand, ms);
+        if (s != GLC_OK) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = cand;
+        }
+      }
+      if (s != GLC_OK) break;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s != GLC_OK) {
+    ctx->policy = saved;
+    return s;
+  }
+  ctx->policy = best;
+  *policy = best;
+  return GLC_OK;
+}
+
+}  // extern "C"

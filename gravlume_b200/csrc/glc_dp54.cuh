@@ -1,0 +1,143 @@
+// Dormand-Prince 5(4) with FSAL, embedded error estimate and Shampine's quartic dense output.
+// Coefficients are the published Dormand-Prince (1980) tableau and the dense-output polynomial the
+// reference's oracle uses (crates/gravlume-reference/src/integrator.rs:6-98); they are compile-time
+// constants here, so every stage combination is an FMA with an immediate operand.
+#pragma once
+
+#include "glc_geometry.cuh"
+
+namespace glc {
+namespace dp {
+// stage matrix A[i][j], i = 1..6 (stage 7 row equals the fifth-order weights B5)
+constexpr double a21 = 1.0 / 5.0;
+constexpr double a31 = 3.0 / 40.0, a32 = 9.0 / 40.0;
+constexpr double a41 = 44.0 / 45.0, a42 = -56.0 / 15.0, a43 = 32.0 / 9.0;
+constexpr double a51 = 19372.0 / 6561.0, a52 = -25360.0 / 2187.0, a53 = 64448.0 / 6561.0, a54 = -212.0 / 729.0;
+constexpr double a61 = 9017.0 / 3168.0, a62 = -355.0 / 33.0, a63 = 46732.0 / 5247.0, a64 = 49.0 / 176.0,
+                 a65 = -5103.0 / 18656.0;
+constexpr double b1 = 35.0 / 384.0, b3 = 500.0 / 1113.0, b4 = 125.0 / 192.0, b5 = -2187.0 / 6784.0, b6 = 11.0 / 84.0;
+// fourth-order weights
+constexpr double c1 = 5179.0 / 57600.0, c3 = 7571.0 / 16695.0, c4 = 393.0 / 640.0, c5 = -92097.0 / 339200.0,
+                 c6 = 187.0 / 2100.0, c7 = 1.0 / 40.0;
+// error weights e = b - c
+constexpr double e1 = b1 - c1, e3 = b3 - c3, e4 = b4 - c4, e5 = b5 - c5, e6 = b6 - c6, e7 = -c7;
+// dense output: y(theta) = y0 + h sum_j (sum_k d_jk theta^(k+1)) K_j (stage 2 has no weight)
+constexpr double d10 = 1.0, d11 = -8048581381.0 / 2820520608.0, d12 = 8663915743.0 / 2820520608.0,
+                 d13 = -12715105075.0 / 11282082432.0;
+constexpr double d31 = 131558114200.0 / 32700410799.0, d32 = -68118460800.0 / 10900136933.0,
+                 d33 = 87487479700.0 / 32700410799.0;
+constexpr double d41 = -1754552775.0 / 470086768.0, d42 = 14199869525.0 / 1410260304.0,
+                 d43 = -10690763975.0 / 1880347072.0;
+constexpr double d51 = 127303824393.0 / 49829197408.0, d52 = -318862633887.0 / 49829197408.0,
+                 d53 = 701980252875.0 / 199316789632.0;
+constexpr double d61 = -282668133.0 / 205662961.0, d62 = 2019193451.0 / 616988883.0,
+                 d63 = -1453857185.0 / 822651844.0;
+constexpr double d71 = 40617522.0 / 29380423.0, d72 = -110615467.0 / 29380423.0, d73 = 69997945.0 / 29380423.0;
+}  // namespace dp
+
+// One attempt. y0 is the state in storage precision S, the stages run in compute precision C.
+// Outputs: inc = h * (fifth-order increment) for the six state components (so y1 = y0 + inc in S),
+// dt = coordinate-time increment, err = embedded error estimate (7 components, time last),
+// k7 = derivative at the end state (FSAL), with r and dr/dlambda there.
+template <class C, class S>
+GLC_HD void dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C inc[6], C& dt, C err[7],
+                        C k7[7], C& r_end, C& vr_end) {
+  using namespace dp;
+  C y0c[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) y0c[c] = C(y0[c]);
+  C k2[7], k3[7], k4[7], k5[7], k6[7], ys[6], rr, vv;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ys[c] = y0c[c] + h * (C(a21) * k1[c]);
+  kn_rhs(k, ys, E, k2, rr, vv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ys[c] = y0c[c] + h * (C(a31) * k1[c] + C(a32) * k2[c]);
+  kn_rhs(k, ys, E, k3, rr, vv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ys[c] = y0c[c] + h * (C(a41) * k1[c] + C(a42) * k2[c] + C(a43) * k3[c]);
+  kn_rhs(k, ys, E, k4, rr, vv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+    ys[c] = y0c[c] + h * (C(a51) * k1[c] + C(a52) * k2[c] + C(a53) * k3[c] + C(a54) * k4[c]);
+  kn_rhs(k, ys, E, k5, rr, vv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+    ys[c] = y0c[c] + h * (C(a61) * k1[c] + C(a62) * k2[c] + C(a63) * k3[c] + C(a64) * k4[c] + C(a65) * k5[c]);
+  kn_rhs(k, ys, E, k6, rr, vv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    inc[c] = h * (C(b1) * k1[c] + C(b3) * k3[c] + C(b4) * k4[c] + C(b5) * k5[c] + C(b6) * k6[c]);
+    ys[c] = y0c[c] + inc[c];
+  }
+  kn_rhs(k, ys, E, k7, r_end, vr_end);
+  dt = h * (C(b1) * k1[6] + C(b3) * k3[6] + C(b4) * k4[6] + C(b5) * k5[6] + C(b6) * k6[6]);
+#pragma unroll
+  for (int c = 0; c < 7; ++c)
+    err[c] = h * (C(e1) * k1[c] + C(e3) * k3[c] + C(e4) * k4[c] + C(e5) * k5[c] + C(e6) * k6[c] + C(e7) * k7[c]);
+}
+
+// Full stage set for dense output (the rare event path). K[0] must hold k1 on entry. The last
+// stage is evaluated at the fifth-order end state, returned in yend with r and dr/dlambda there.
+template <class T>
+GLC_HD void dp5_stages(const KN<T>& k, const T y0[6], T E, T h, T K[7][7], T yend[6], T& r_end, T& vr_end) {
+  using namespace dp;
+  const double A[7][6] = {{0, 0, 0, 0, 0, 0},       {a21, 0, 0, 0, 0, 0},       {a31, a32, 0, 0, 0, 0},
+                          {a41, a42, a43, 0, 0, 0}, {a51, a52, a53, a54, 0, 0}, {a61, a62, a63, a64, a65, 0},
+                          {b1, 0, b3, b4, b5, b6}};
+  T ys[6], rr, vv;
+#pragma unroll
+  for (int s = 1; s < 7; ++s) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      T w = T(0);
+#pragma unroll
+      for (int j = 0; j < s; ++j) w += T(A[s][j]) * K[j][c];
+      ys[c] = y0[c] + h * w;
+    }
+    kn_rhs(k, ys, E, K[s], rr, vv);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) yend[c] = ys[c];
+  r_end = rr;
+  vr_end = vv;
+}
+
+template <class T>
+GLC_HD void dense_weights(T th, T w[7]) {
+  using namespace dp;
+  const T p1 = th, p2 = th * th, p3 = p2 * th, p4 = p2 * p2;
+  w[0] = T(d10) * p1 + T(d11) * p2 + T(d12) * p3 + T(d13) * p4;
+  w[1] = T(0);
+  w[2] = T(d31) * p2 + T(d32) * p3 + T(d33) * p4;
+  w[3] = T(d41) * p2 + T(d42) * p3 + T(d43) * p4;
+  w[4] = T(d51) * p2 + T(d52) * p3 + T(d53) * p4;
+  w[5] = T(d61) * p2 + T(d62) * p3 + T(d63) * p4;
+  w[6] = T(d71) * p2 + T(d72) * p3 + T(d73) * p4;
+}
+
+// Dense state (six components) and coordinate-time increment at theta.
+template <class T>
+GLC_HD void dense_eval(const T y0[6], T h, const T K[7][7], T th, T y[6], T& dt) {
+  T w[7];
+  dense_weights(th, w);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) s += w[j] * K[j][c];
+    if (c < 6) y[c] = y0[c] + h * s;
+    else dt = h * s;
+  }
+}
+
+template <class T>
+GLC_HD T dense_component(const T y0[6], T h, const T K[7][7], T th, int c) {
+  T w[7];
+  dense_weights(th, w);
+  T s = T(0);
+#pragma unroll
+  for (int j = 0; j < 7; ++j) s += w[j] * K[j][c];
+  return y0[c] + h * s;
+}
+
+}  // namespace glc

@@ -1,0 +1,263 @@
+// Kerr-Newman geometry and the reduced Hamilton right-hand side in Cartesian Kerr-Schild
+// coordinates, templated on the arithmetic type (float / double) and compiled for both the
+// device and the host (host builds back glc_rhs_host and the CPU checks).
+//
+// Metric: g^{mu nu} = eta^{mu nu} - f l^mu l^nu with l^mu = (-1, l_x, l_y, l_z), M = 1,
+//   r^2 = (b + sqrt(b^2 + 4 a^2 z^2)) / 2, b = x^2 + y^2 + z^2 - a^2 (conjugate root when b < 0),
+//   f = (2 r - Q^2) r^2 / (r^4 + a^2 z^2),
+//   l = s ((r x + s a y) / (r^2 + a^2), (r y - s a x) / (r^2 + a^2), z / r), s = +1 ingoing, -1 outgoing.
+// With q = E + l.p (E = -p_t) the exact reduced system is
+//   x' = p - f q l,  p' = f q w + q^2 grad(f) / 2,  t' = E + f q,   w_i = p_j d_i l_j = e_i + C d_i r,
+//   e = ((s r p_x - a p_y) / A, (a p_x + s r p_y) / A, s p_z / r), A = r^2 + a^2,
+//   C = [(s x - 2 r l_x) p_x + (s y - 2 r l_y) p_y] / A - s z p_z / r^2.
+// This is the contraction of the full null-vector Jacobian that the reference's binary64 oracle
+// builds explicitly (crates/gravlume-domain/src/spacetime.rs:492-582, hamiltonian_rhs 305-338);
+// the reference derives the same contracted form in docs/physics.md section 4. The state carries
+// (x, y, z, p_x, p_y, p_z) and the relative coordinate time; E is constant per ray.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define GLC_HD __host__ __device__ __forceinline__
+#else
+#define GLC_HD inline
+#endif
+
+namespace glc {
+
+// ---------------------------------------------------------------- precision helpers
+GLC_HD float g_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(x);
+#else
+  return 1.0f / std::sqrt(x);
+#endif
+}
+GLC_HD double g_rsqrt(double x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrt(x);
+#else
+  return 1.0 / std::sqrt(x);
+#endif
+}
+GLC_HD float g_rcp(float x) {
+#if defined(__CUDA_ARCH__)
+  return __frcp_rn(x);
+#else
+  return 1.0f / x;
+#endif
+}
+GLC_HD double g_rcp(double x) {
+#if defined(__CUDA_ARCH__)
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+GLC_HD float g_sqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return sqrtf(x);
+#else
+  return std::sqrt(x);
+#endif
+}
+GLC_HD double g_sqrt(double x) {
+#if defined(__CUDA_ARCH__)
+  return sqrt(x);
+#else
+  return std::sqrt(x);
+#endif
+}
+#if defined(__CUDA_ARCH__)
+GLC_HD float g_abs(float x) { return fabsf(x); }
+GLC_HD double g_abs(double x) { return fabs(x); }
+GLC_HD float g_max(float a, float b) { return fmaxf(a, b); }
+GLC_HD double g_max(double a, double b) { return fmax(a, b); }
+GLC_HD float g_min(float a, float b) { return fminf(a, b); }
+GLC_HD double g_min(double a, double b) { return fmin(a, b); }
+GLC_HD bool g_finite(float x) { return isfinite(x); }
+GLC_HD bool g_finite(double x) { return isfinite(x); }
+GLC_HD bool g_signbit(float x) { return signbit(x); }
+GLC_HD bool g_signbit(double x) { return signbit(x); }
+GLC_HD float g_floor(float x) { return floorf(x); }
+GLC_HD double g_floor(double x) { return floor(x); }
+GLC_HD float g_atan2(float y, float x) { return atan2f(y, x); }
+GLC_HD double g_atan2(double y, double x) { return atan2(y, x); }
+GLC_HD float g_acos(float x) { return acosf(x); }
+GLC_HD double g_acos(double x) { return acos(x); }
+#else
+GLC_HD float g_abs(float x) { return std::fabs(x); }
+GLC_HD double g_abs(double x) { return std::fabs(x); }
+GLC_HD float g_max(float a, float b) { return std::fmax(a, b); }
+GLC_HD double g_max(double a, double b) { return std::fmax(a, b); }
+GLC_HD float g_min(float a, float b) { return std::fmin(a, b); }
+GLC_HD double g_min(double a, double b) { return std::fmin(a, b); }
+GLC_HD bool g_finite(float x) { return std::isfinite(x); }
+GLC_HD bool g_finite(double x) { return std::isfinite(x); }
+GLC_HD bool g_signbit(float x) { return std::signbit(x); }
+GLC_HD bool g_signbit(double x) { return std::signbit(x); }
+GLC_HD float g_floor(float x) { return std::floor(x); }
+GLC_HD double g_floor(double x) { return std::floor(x); }
+GLC_HD float g_atan2(float y, float x) { return std::atan2(y, x); }
+GLC_HD double g_atan2(double y, double x) { return std::atan2(y, x); }
+GLC_HD float g_acos(float x) { return std::acos(x); }
+GLC_HD double g_acos(double x) { return std::acos(x); }
+#endif
+// err^(-1/5) for the step controller.
+GLC_HD float g_pow_m02(float x) {
+#if defined(__CUDA_ARCH__)
+  return exp2f(-0.2f * __log2f(x));
+#else
+  return std::pow(x, -0.2f);
+#endif
+}
+GLC_HD double g_pow_m02(double x) {
+#if defined(__CUDA_ARCH__)
+  return pow(x, -0.2);
+#else
+  return std::pow(x, -0.2);
+#endif
+}
+
+// ---------------------------------------------------------------- spacetime constants
+template <class T>
+struct KN {
+  T a, a2, s, sa, q2;  // spin, spin^2, chart sign, s*a, charge^2  (M = 1)
+};
+
+template <class T, class U>
+GLC_HD KN<T> kn_cast(const KN<U>& k) {
+  return KN<T>{T(k.a), T(k.a2), T(k.s), T(k.sa), T(k.q2)};
+}
+
+enum GeomStatus : int { kGeomOk = 0, kGeomRing = 2, kGeomChart = 3, kGeomDenominator = 4 };
+
+// Kerr-Schild radius squared from Cartesian position (stable root selection).
+template <class T>
+GLC_HD T kn_radius_squared(const KN<T>& k, T x, T y, T z, int& status) {
+  const T R2 = x * x + y * y + z * z;
+  const T b = R2 - k.a2;
+  const T az2 = k.a2 * z * z;
+  const T sq = g_sqrt(b * b + T(4) * az2);
+  T r2;
+  if (b >= T(0)) {
+    r2 = T(0.5) * (b + sq);
+  } else {
+    r2 = T(2) * az2 / (sq - b);
+  }
+  status = r2 > T(0) ? kGeomOk : (b == T(0) ? kGeomRing : kGeomChart);
+  return r2;
+}
+
+template <class T>
+GLC_HD T kn_radius(const KN<T>& k, T x, T y, T z, int& status) {
+  const T r2 = kn_radius_squared(k, x, y, z, status);
+  return g_sqrt(r2);
+}
+
+// Reduced right-hand side. y = (x, y, z, p_x, p_y, p_z); d = (x', y', z', p_x', p_y', p_z', t').
+// Also returns r and the radial velocity dr/dlambda = grad(r) . x'. Non-finite values propagate
+// as NaN into the step's error norm, which the stepper turns into a numerical failure.
+template <class T>
+GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_out) {
+  const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
+  const T R2 = x * x + yy * yy + z * z;
+  const T b = R2 - k.a2;
+  const T az2 = k.a2 * z * z;
+  const T sq = g_sqrt(b * b + T(4) * az2);
+  T r2;
+  if (b >= T(0)) {
+    r2 = T(0.5) * (b + sq);
+  } else {
+    r2 = T(2) * az2 * g_rcp(sq - b);
+  }
+  const T inv_r = g_rsqrt(r2);
+  const T r = r2 * inv_r;
+  const T inv_r2 = inv_r * inv_r;
+  const T A = r2 + k.a2;
+  const T inv_A = g_rcp(A);
+  const T sigma = r2 + az2 * inv_r2;  // (r^4 + a^2 z^2) / r^2
+  const T inv_sigma = g_rcp(sigma);
+  // grad r = (x r, y r, z A / r) / sigma
+  const T rs = r * inv_sigma;
+  const T grx = x * rs, gry = yy * rs, grz = z * A * inv_r * inv_sigma;
+  // f = (2 r - Q^2) / sigma ; grad f = (2 grad r - f grad sigma) / sigma,
+  // grad sigma = 2 (r - a^2 z^2 / r^3) grad r + (0, 0, 2 a^2 z / r^2)
+  const T f = (T(2) * r - k.q2) * inv_sigma;
+  const T srf = T(2) * (r - az2 * inv_r2 * inv_r);
+  const T c1 = (T(2) - f * srf) * inv_sigma;
+  const T gfx = c1 * grx, gfy = c1 * gry;
+  const T gfz = c1 * grz - f * (T(2) * k.a2 * z * inv_r2) * inv_sigma;
+  // null vector l
+  const T lx = k.s * (r * x + k.sa * yy) * inv_A;
+  const T ly = k.s * (r * yy - k.sa * x) * inv_A;
+  const T lz = k.s * z * inv_r;
+  const T q = E + lx * px + ly * py + lz * pz;
+  const T fq = f * q;
+  const T vx = px - fq * lx, vy = py - fq * ly, vz = pz - fq * lz;
+  // w = e + C grad r
+  const T sr = k.s * r;
+  const T ex = (sr * px - k.a * py) * inv_A;
+  const T ey = (k.a * px + sr * py) * inv_A;
+  const T ez = k.s * pz * inv_r;
+  const T C = ((k.s * x - T(2) * r * lx) * px + (k.s * yy - T(2) * r * ly) * py) * inv_A - k.s * z * pz * inv_r2;
+  const T hq2 = T(0.5) * q * q;
+  d[0] = vx;
+  d[1] = vy;
+  d[2] = vz;
+  d[3] = fq * (ex + C * grx) + hq2 * gfx;
+  d[4] = fq * (ey + C * gry) + hq2 * gfy;
+  d[5] = fq * (ez + C * grz) + hq2 * gfz;
+  d[6] = E + fq;
+  r_out = r;
+  vr_out = grx * vx + gry * vy + grz * vz;
+}
+
+// Conserved quantities and the normalized null residual (the reference's drift diagnostics,
+// crates/gravlume-domain/src/spacetime.rs:345-401 and numerics.rs:3-35). Carter's constant uses
+// the axis-regular Cartesian form
+//   Q = (z^2 / r^2) (A P_perp^2 - a^2 E^2) - 2 z S p_z + (r^2 rho^2 / A) p_z^2,
+//   S = x p_x + y p_y, P_perp^2 = p_x^2 + p_y^2, rho^2 = x^2 + y^2,
+// which equals the oracle's trigonometric form p_theta^2 + cos^2(theta)(L_z^2/sin^2 - a^2 E^2).
+template <class T>
+struct Invariants {
+  T lz, carter, null_residual;
+};
+
+template <class T>
+GLC_HD Invariants<T> kn_invariants(const KN<T>& k, const T y[6], T E, T r) {
+  const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
+  Invariants<T> out;
+  out.lz = x * py - yy * px;
+  const T r2 = r * r;
+  const T A = r2 + k.a2;
+  const T rho2 = x * x + yy * yy;
+  const T S = x * px + yy * py;
+  const T pp2 = px * px + py * py;
+  out.carter = (z * z / r2) * (A * pp2 - k.a2 * E * E) - T(2) * z * S * pz + (r2 * rho2 / A) * pz * pz;
+  // g^{mu nu} p_mu p_nu with g^{mu nu} = eta - f l l, p = (-E, p_x, p_y, p_z), l = (-1, l_x, l_y, l_z).
+  const T inv_r = T(1) / r;
+  const T sigma = r2 + k.a2 * z * z / r2;
+  const T f = (T(2) * r - k.q2) / sigma;
+  const T inv_A = T(1) / A;
+  const T l[4] = {T(-1), k.s * (r * x + k.sa * yy) * inv_A, k.s * (r * yy - k.sa * x) * inv_A, k.s * z * inv_r};
+  const T p[4] = {-E, px, py, pz};
+  T sum = T(0), norm = T(0);
+  for (int i = 0; i < 4; ++i) {
+    for (int j = 0; j < 4; ++j) {
+      const T eta = i == j ? (i == 0 ? T(-1) : T(1)) : T(0);
+      const T m = eta - f * l[i] * l[j];
+      const T term = m * p[i] * p[j];
+      sum += term;
+      norm += g_abs(term);
+    }
+  }
+  // |sum| / norm * min(norm, 1): the reference's scale-normalized residual
+  // (numerics.rs:3-35) with its overflow-safe product collapsed for finite moderate inputs.
+  out.null_residual = norm > T(0) ? g_abs(sum) / norm * g_min(norm, T(1)) : T(0);
+  return out;
+}
+
+}  // namespace glc

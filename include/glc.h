@@ -1,0 +1,261 @@
+/*
+ * glc.h - C ABI of the B200-native Kerr-Newman null-geodesic trace (Gravlume hot path).
+ *
+ * Plain C: pointers, sizes and PODs only; no CUDA, C++ or torch types cross this boundary (a
+ * CUDA stream is passed as `void*`). All traces are asynchronous on the caller's stream; results
+ * land in caller-owned device arrays. Nothing here aborts the process: every failure is a
+ * glc_status, and glc_last_error_string() describes the last one on the calling thread.
+ *
+ * The entry points replace the reference's trace boundary (paths are within romeoahmed/gravlume):
+ *   glc_scene_pack   <- TraceUniforms::from_observation_with_surface
+ *                       (crates/gravlume-render/src/trace/input.rs:45-131), with the domain
+ *                       validation of PhysicalScene::new / StationaryObserverInput::build
+ *                       (crates/gravlume-domain/src/scene.rs:112-143, observer.rs:67-103)
+ *   glc_create       <- TracePipeline::new (crates/gravlume-render/src/trace.rs:320-327)
+ *   glc_trace        <- TracePipeline::encode_batch (trace.rs:701-710) for image cameras, and
+ *                       GeodesicTracer::trace / GeodesicBatch::trace_ordered
+ *                       (crates/gravlume-reference/src/geodesic.rs:53-62, batch.rs:31-43) for
+ *                       explicit ray lists
+ *   glc_results      <- GeometricSample (src/shaders/trace_protocol.wgsl:72-83) widened to the
+ *                       reference outcome (crates/gravlume-reference/src/outcome.rs:425-436)
+ *   glc_policy       <- ReferencePolicy (crates/gravlume-reference/src/policy.rs:26-66)
+ *                       plus the precision mode and launch shape of this implementation
+ */
+#ifndef GLC_H
+#define GLC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GLC_ABI_VERSION 1
+
+typedef enum glc_status {
+  GLC_OK = 0,
+  GLC_ERR_INVALID_ARGUMENT = 1,   /* null pointer, bad size, bad enum */
+  GLC_ERR_CUDA = 2,               /* a CUDA runtime call failed (see glc_last_error_string) */
+  GLC_ERR_NON_FINITE = 3,         /* GpuTraceInputError::NonFinite / ValidationIssueCode::NonFinite */
+  GLC_ERR_NON_POSITIVE = 4,       /* mass, frequency or radius not positive */
+  GLC_ERR_NON_NORMALIZED = 5,     /* observer frequency != 1 within 32 eps (input.rs:61-63) */
+  GLC_ERR_EXTREMALITY_CHANGED = 6,/* normalization by M changed the extremality (input.rs:84-91) */
+  GLC_ERR_NON_STATIONARY = 7,     /* observer needs g_tt < 0 (observer.rs:80-86) */
+  GLC_ERR_DEGENERATE_FRAME = 8,   /* target/up do not define a tetrad (observer.rs:116-151) */
+  GLC_ERR_SURFACE_OUTSIDE_ESCAPE = 9, /* events.rs:73-78 */
+  GLC_ERR_INVALID_SURFACE = 10,   /* events.rs:66-72 */
+  GLC_ERR_INVALID_VIEW = 11,      /* view.rs:349-363 */
+  GLC_ERR_TIMEOUT = 12,           /* a bounded device wait ran out */
+  GLC_ERR_CAPACITY = 13,          /* request exceeds a stated maximum */
+  GLC_ERR_NO_DEVICE = 14,
+  GLC_ERR_UNSUPPORTED = 15
+} glc_status;
+
+/* Arithmetic of the stepper. FP32: state and right-hand side in binary32. MIXED: binary64 state
+ * accumulators, binary32 right-hand side and stage combination, binary64 steps inside the
+ * near-hole shell, binary64 event root-finding and a binary64 null-constraint renormalisation of
+ * the final momentum. FP64: binary64 throughout. */
+typedef enum glc_precision { GLC_FP32 = 0, GLC_MIXED = 1, GLC_FP64 = 2 } glc_precision;
+
+typedef enum glc_chart { GLC_CHART_INGOING = 0, GLC_CHART_OUTGOING = 1 } glc_chart;
+
+/* Termination discriminants: 1-7 are the reference's TraceTermination
+ * (crates/gravlume-render/src/trace.rs:957-967); 8 is the adaptive stepper's consecutive-reject
+ * limit (ReferenceTerminal::RejectExhaustion, outcome.rs:303). */
+typedef enum glc_termination {
+  GLC_TERM_NONE = 0,
+  GLC_TERM_HORIZON = 1,
+  GLC_TERM_ESCAPE = 2,
+  GLC_TERM_SINGULARITY = 3,
+  GLC_TERM_STEP_EXHAUSTION = 4,
+  GLC_TERM_NUMERICAL_FAILURE = 5,
+  GLC_TERM_UNCERTAIN = 6,
+  GLC_TERM_SURFACE = 7,
+  GLC_TERM_REJECT_EXHAUSTION = 8
+} glc_termination;
+
+/* NumericalFailure kinds (outcome.rs:129-136), in bits 8..11 of glc_results.code.x. */
+typedef enum glc_failure {
+  GLC_FAIL_NONE = 0, GLC_FAIL_NON_FINITE = 1, GLC_FAIL_RING = 2, GLC_FAIL_CHART_BOUNDARY = 3,
+  GLC_FAIL_DENOMINATOR = 4, GLC_FAIL_MINIMUM_STEP = 5
+} glc_failure;
+
+/* Physical scene, observer, view and events in the reference's terms
+ * (PhysicalSceneInput scene.rs:11-36, StationaryObserverInput observer.rs:9-31,
+ *  PerspectiveView view.rs:343-370, EventConfiguration events.rs:17-84,
+ *  EquatorialCircularEmitter emission.rs:30-41). */
+typedef struct glc_scene_input {
+  double mass, spin, charge;      /* M, a = J/M, Q in geometric units */
+  int32_t chart;                  /* glc_chart */
+  int32_t has_surface;            /* install the equatorial Keplerian surface */
+  double observer_txyz[4];        /* observer event, Cartesian Kerr-Schild */
+  double target_txyz[4];          /* look-at event */
+  double up_hint_xyz[3];
+  double measured_frequency;      /* must be 1 (reference-v1 normalization) */
+  uint32_t width, height;         /* pinhole view */
+  double vertical_fov;            /* radians, in (0, pi) */
+  double escape_radius;           /* > 0: escape sphere r = R (reference baseline: 200 M) */
+  double surface_inner, surface_outer; /* inclusive radial interval of the surface */
+  double intensity_at_six;        /* bolometric I(6 M) of the inverse-cube emitter */
+  double horizon_offset;          /* capture at r = r_+ + offset (reference: 0) */
+} glc_scene_input;
+
+/* Device-ready packed scene, normalized to M = 1 (the analogue of TraceUniforms, kept in
+ * binary64). Produced by glc_scene_pack; treat as read-only. */
+typedef struct glc_scene {
+  double spin, charge, chart_sign, mass_scale;
+  double outer_horizon;           /* r_+, or -1 without a horizon */
+  double horizon_event_radius;    /* r_+ + offset */
+  double escape_radius;           /* 0 when not installed */
+  double surface_inner, surface_outer, intensity_at_six;
+  double photon_shell_radius;     /* outer (retrograde) equatorial photon orbit radius */
+  double isco_prograde;           /* prograde ISCO radius (informational) */
+  double observer_txyz[4];
+  double four_velocity[4], image_right[4], image_up[4], arrival[4];
+  double metric_covariant[16];    /* g_{mu nu} at the observer */
+  double frequency;
+  double tangent_half_fov;
+  uint32_t width, height;
+  int32_t extremality;            /* 0 subextremal, 1 extremal, 2 superextremal */
+  int32_t has_horizon, has_escape, has_surface;
+  int32_t reserved[2];
+} glc_scene;
+
+/* Step policy: ReferencePolicy fields (policy.rs:26-66) + precision + launch shape. */
+typedef struct glc_policy {
+  double position_rtol, position_atol, momentum_rtol, momentum_atol;
+  double initial_step, minimum_step, maximum_step;
+  double safety, minimum_factor, maximum_factor;
+  uint64_t maximum_accepted_steps;
+  uint32_t maximum_consecutive_rejects;
+  int32_t precision;              /* glc_precision */
+  double event_affine_tolerance, event_tie_tolerance, event_arming_band, singularity_guard;
+  double mixed_shell_factor;      /* MIXED: binary64 steps while r < factor * photon shell radius */
+  uint32_t renormalize_null;      /* MIXED: renormalize the final momentum onto H = 0 */
+  uint32_t persistent;            /* 1: persistent work-queue kernel, 0: one thread per ray */
+  uint32_t block_threads;         /* threads per block (multiple of 32) */
+  uint32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = occupancy) */
+  uint32_t tile_w, tile_h;        /* pixel tile a warp's consecutive rays cover */
+  uint32_t refill_interval;       /* persistent: steps between warp refills of finished lanes */
+  uint32_t rays_per_grab;         /* persistent: rays a warp takes from the queue per refill (>= 32) */
+} glc_policy;
+
+typedef enum glc_camera_kind {
+  GLC_CAMERA_PINHOLE = 0,         /* PerspectiveView sight plane (view.rs:408-424) */
+  GLC_CAMERA_EQUIRECT = 1,        /* full-sphere longitude/latitude map in the observer frame */
+  GLC_CAMERA_RAYLIST = 2          /* explicit initial states (t,x,y,z,p_t,p_x,p_y,p_z) */
+} glc_camera_kind;
+
+typedef struct glc_camera {
+  int32_t kind;                   /* glc_camera_kind */
+  int32_t scene_index;            /* index into the scenes array of the call */
+  uint32_t width, height;         /* image size (PINHOLE: must equal the scene's view) */
+  double subpixel_x, subpixel_y;  /* sample offset inside the pixel, [0, 1] */
+  const double* ray_states;       /* RAYLIST: device pointer, n_rays * 8 doubles */
+  uint64_t n_rays;                /* RAYLIST: number of rays (images: ignored) */
+  double affine_direction;        /* RAYLIST: +1 or -1 (images trace backward, -1) */
+  uint64_t result_offset;         /* first result slot of this camera */
+} glc_camera;
+
+/* Caller-owned device SoA, one 16-byte element per ray in each array (128-bit stores). Any
+ * pointer may be NULL to skip that field. Lengths: >= max(result_offset + rays of camera).
+ *   code.x  termination | failure << 8 | event candidates << 12 | (polar side + 1) << 16
+ *           | flags << 20 (bit 20: shell steps taken in binary64; bit 21: null renormalized)
+ *   code.y  accepted steps, code.z rejected steps, code.w binary64 steps (MIXED)
+ *   branch  radial turnings, equatorial crossings, azimuth winding, has turning radius
+ *   escape  (polar angle, azimuth) of the unit coordinate direction at escape (NaN otherwise)
+ *   surface (source radius, source azimuth) at a surface hit (NaN otherwise)
+ *   redshift_time (g = nu_obs / nu_em at a surface hit or NaN, coordinate travel time)
+ *   event   (normalized event residual, affine parameter at termination)
+ *   drift_a (max normalized null residual, max relative energy drift)
+ *   drift_b (max relative L_z drift, max relative Carter drift)
+ *   turning (minimum turning radius or NaN, azimuth advance)
+ *   position_xy / position_zr (final x, y) / (final z, final Kerr-Schild radius) */
+typedef struct glc_u32x4 { uint32_t x, y, z, w; } glc_u32x4;
+typedef struct glc_i32x4 { int32_t x, y, z, w; } glc_i32x4;
+typedef struct glc_f64x2 { double x, y; } glc_f64x2;
+
+typedef struct glc_results {
+  glc_u32x4* code;
+  glc_i32x4* branch;
+  glc_f64x2* escape;
+  glc_f64x2* surface;
+  glc_f64x2* redshift_time;
+  glc_f64x2* event;
+  glc_f64x2* drift_a;
+  glc_f64x2* drift_b;
+  glc_f64x2* turning;
+  glc_f64x2* position_xy;
+  glc_f64x2* position_zr;
+} glc_results;
+
+typedef struct glc_ctx glc_ctx;
+typedef struct glc_graph glc_graph;
+
+typedef struct glc_launch_stats {
+  uint64_t kernel_launches;       /* kernels this context launched since creation */
+  uint64_t last_rays;             /* rays in the last trace */
+  uint32_t last_grid, last_block; /* launch shape of the last trace kernel */
+  uint32_t last_persistent;       /* 1 if the last trace used the work queue */
+  uint32_t sm_count;
+} glc_launch_stats;
+
+/* ---- version and errors ---------------------------------------------------------------- */
+int glc_abi_version(void);
+const char* glc_last_error_string(void);
+const char* glc_status_string(glc_status status);
+
+/* ---- scenes and policies (host only; no device needed) ---------------------------------- */
+glc_status glc_scene_pack(const glc_scene_input* input, glc_scene* out);
+/* preset: 0 reference-regular-v1, 1 reference-strict-v1, 2 frame policy of the precision mode. */
+glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out);
+/* Prograde ISCO radius of Kerr-Newman in units of M (spin, charge in units of M). */
+glc_status glc_prograde_isco(double spin, double charge, double* out);
+/* Algorithmic operation model of the kernel (counted from the same templated source on the host):
+ * out[0] flops per right-hand-side evaluation (FMA = 2), out[1] special-function ops (rcp, sqrt,
+ * rsqrt) per evaluation, out[2] flops per attempted DP5(4) step, out[3] special ops per step. */
+glc_status glc_flop_model(double out4[4]);
+/* Host evaluation of the device right-hand side (the same template code), for checks:
+ * state = (x, y, z, p_x, p_y, p_z), energy = -p_t; out = (x', y', z', p_x', p_y', p_z', t'). */
+glc_status glc_rhs_host(const glc_scene* scene, const double state6[6], double energy, int32_t precision,
+                        double out7[7]);
+
+/* ---- context ----------------------------------------------------------------------------- */
+glc_status glc_create(int32_t device, glc_ctx** out);
+glc_status glc_destroy(glc_ctx* ctx);
+glc_status glc_set_policy(glc_ctx* ctx, const glc_policy* policy);
+glc_status glc_get_policy(const glc_ctx* ctx, glc_policy* out);
+glc_status glc_get_stats(const glc_ctx* ctx, glc_launch_stats* out);
+
+/* ---- forward trace ----------------------------------------------------------------------- */
+/* Number of result slots the cameras need (max over result_offset + rays). */
+glc_status glc_result_slots(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                            int32_t n_cameras, uint64_t* out);
+/* Trace every camera's rays; stream-ordered and asynchronous. Scenes/cameras are host arrays
+ * (copied into the context's device job table on `stream`); results are device pointers. */
+glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                     int32_t n_cameras, const glc_results* out, void* stream);
+/* End-to-end convenience over host buffers: copies RAYLIST states host->device, traces, and
+ * copies every non-NULL result array device->host. Synchronous. */
+glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                          int32_t n_cameras, const glc_results* host_out);
+
+/* ---- CUDA graphs (per-frame replay of the job-table copy, queue reset and trace launch) ---- */
+glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                             int32_t n_cameras, const glc_results* out, void* stream, glc_graph** graph);
+glc_status glc_graph_launch(glc_graph* graph, void* stream);
+glc_status glc_graph_destroy(glc_graph* graph);
+
+/* ---- autotuner ----------------------------------------------------------------------------- */
+/* Times candidate launch shapes (tile shape, rays per grab, refill interval, block size) on the
+ * given job and writes the fastest into *policy (and the context). out may be scratch results. */
+glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                        int32_t n_cameras, const glc_results* out, void* stream, int32_t repeats,
+                        glc_policy* policy);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLC_H */

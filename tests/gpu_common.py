@@ -1,0 +1,75 @@
+"""Shared workload definitions and oracle comparisons for the GPU parity tests."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+import gravlume_b200 as G
+import oracle as O
+
+F = O.F
+
+
+def config1_observation(width=256, height=256, spin=0.9, charge=0.3, incl_deg=75.0, r_obs=50.0, chart=1,
+                        escape=1000.0, fov_deg=30.0, surface=True, horizon_offset=1e-3):
+    """Kerr-Newman a=0.9, Q=0.3 observer at r=50 M, i=75 deg, 30 deg FOV; escape 1000 M, capture at
+    r_+ + 1e-3, Keplerian surface from the prograde ISCO to 20 M (the CPU-runnable benchmark case)."""
+    surf = G.EquatorialSurface(G.prograde_isco(spin, charge), 20.0) if surface else None
+    return G.Observation.from_oblate(r_obs, math.radians(incl_deg), 0.0, spin=spin, charge=charge, chart=chart,
+                                     width=width, height=height, vertical_fov=math.radians(fov_deg),
+                                     escape_radius=escape, surface=surf, horizon_offset=horizon_offset)
+
+
+def oracle_for(obs: G.Observation):
+    sc = obs.packed
+    osc = O.scene(mass=obs.mass, spin=obs.spin, charge=obs.charge, chart=int(obs.chart),
+                  observer_txyz=obs.observer_txyz, target=obs.target_txyz, up_hint=obs.up_hint_xyz,
+                  width=obs.width, height=obs.height, vertical_fov=obs.vertical_fov)
+    surf = (obs.surface.inner_radius, obs.surface.outer_radius) if obs.surface else None
+    ev = O.events(escape_radius=obs.escape_radius if obs.escape_radius > 0 else None, surface=surf,
+                  horizon_offset=obs.horizon_offset,
+                  intensity_at_six=obs.surface.intensity_at_six if obs.surface else 1.0)
+    return osc, ev, sc
+
+
+def seeded_pixels(width, height, n, seed):
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(width * height, size=min(n, width * height), replace=False))
+    return idx % width, idx // width
+
+
+def unit(theta, phi):
+    return np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], axis=-1)
+
+
+def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
+    """Per-observable max error of GPU rays `sel` against oracle rows `ref` (matching classes only)."""
+    gt = gpu["termination"][sel]
+    ot = ref[:, F["termination"]].astype(int)
+    same = gt == ot
+    rep = {"n": int(sel.size), "class_mismatch": int((~same).sum())}
+    esc = same & (ot == G.Termination.ESCAPE)
+    if esc.any():
+        d = np.stack([ref[esc, F["escape_dx"]], ref[esc, F["escape_dy"]], ref[esc, F["escape_dz"]]], axis=1)
+        v = unit(gpu["escape_theta"][sel][esc], gpu["escape_phi"][sel][esc])
+        rep["escape_direction_rad"] = float(np.max(np.arccos(np.clip(np.sum(d * v, axis=1), -1.0, 1.0))))
+    srf = same & (ot == G.Termination.EQUATORIAL_SURFACE)
+    if srf.any():
+        g0 = ref[srf, F["frequency_ratio"]]
+        rep["g_rel"] = float(np.max(np.abs(gpu["frequency_ratio"][sel][srf] - g0) / g0))
+        rep["hit_radius"] = float(np.max(np.abs(gpu["source_radius"][sel][srf] - ref[srf, F["source_radius"]])))
+        dphi = gpu["source_azimuth"][sel][srf] - ref[srf, F["source_azimuth"]]
+        rep["source_azimuth"] = float(np.max(np.abs((dphi + np.pi) % (2 * np.pi) - np.pi)))
+    if same.any():
+        rep["travel_time"] = float(np.max(np.abs(gpu["travel_time"][sel][same] - ref[same, F["travel_time"]])))
+        ev = same & np.isfinite(ref[:, F["event_residual"]])
+        if ev.any():
+            rep["event_residual_gpu_max"] = float(np.nanmax(gpu["event_residual"][sel][ev]))
+        for k in ("max_null_residual", "max_lz_drift", "max_carter_drift"):
+            rep[k] = float(np.max(np.abs(gpu[k][sel][same] - ref[same, F[k]])))
+        rep["radial_turnings_mismatch"] = int((gpu["radial_turnings"][sel][same] != ref[same, F["radial_turnings"]]).sum())
+        rep["equatorial_crossings_mismatch"] = int(
+            (gpu["equatorial_crossings"][sel][same] != ref[same, F["equatorial_crossings"]]).sum())
+    return rep
