@@ -112,7 +112,9 @@ def fp32_fma_peak_tflops(sm_count: int, sm_mhz: float) -> float:
     return sm_count * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
-def make_observation(G, width=WIDTH, height=HEIGHT):
+def make_observation(G, width=None, height=None):
+    width = width or WIDTH
+    height = height or HEIGHT
     isco = G.prograde_isco(SPIN, CHARGE)
     return G.Observation.from_oblate(R_OBS, math.radians(INCL_DEG), 0.0, spin=SPIN, charge=CHARGE,
                                      chart=G.KerrSchildChart.OUTGOING, width=width, height=height,
@@ -231,8 +233,8 @@ def run_gpu(args) -> None:
     results = G.TraceResults(WIDTH * HEIGHT, dev)
     stream = torch.cuda.current_stream()
     if args.autotune:
-        small = make_observation(G, WIDTH // 4, HEIGHT // 4)
-        pipe.autotune([small.pack()], [G.image_camera(0, WIDTH // 4, HEIGHT // 4)], repeats=1)
+        small = make_observation(G, max(WIDTH // 4, 64), max(HEIGHT // 4, 64))
+        pipe.autotune([small.pack()], [G.image_camera(0, small.width, small.height)], repeats=1)
     policy = pipe.policy.as_dict()
     flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
@@ -370,7 +372,11 @@ def main() -> None:
                     help="pixels of the frame traced by the CPU oracle (baseline and error report)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch from an ncu capture, reported as roofline.traffic")
+    ap.add_argument("--width", type=int, default=WIDTH, help="frame width (smaller frames for profiling)")
+    ap.add_argument("--height", type=int, default=HEIGHT, help="frame height")
     args = ap.parse_args()
+    global WIDTH, HEIGHT
+    WIDTH, HEIGHT = args.width, args.height
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -35,13 +35,19 @@ constexpr double d61 = -282668133.0 / 205662961.0, d62 = 2019193451.0 / 61698888
 constexpr double d71 = 40617522.0 / 29380423.0, d72 = -110615467.0 / 29380423.0, d73 = 69997945.0 / 29380423.0;
 }  // namespace dp
 
+struct Tolerance {
+  double pos_rtol, pos_atol, mom_rtol, mom_atol;
+};
+
 // One attempt. y0 is the state in storage precision S, the stages run in compute precision C.
-// Outputs: inc = h * (fifth-order increment) for the six state components (so y1 = y0 + inc in S),
-// dt = coordinate-time increment, err = embedded error estimate (7 components, time last),
-// k7 = derivative at the end state (FSAL), with r and dr/dlambda there.
-template <class C, class S>
-GLC_HD void dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C inc[6], C& dt, C err[7],
-                        C k7[7], C& r_end, C& vr_end) {
+// Returns the grouped infinity norm of the embedded error (the reference's error_norm with the
+// relative coordinate time in the time slot, crates/gravlume-reference/src/policy.rs:137-158 and
+// geodesic.rs:158-165). Outputs: inc = fifth-order increment of the six state components
+// (y1 = y0 + inc in S), dt = coordinate-time increment, k7 = derivative at the end (FSAL) with
+// r, dr/dlambda and the invariants there; `finite` is false if anything overflowed or became NaN.
+template <class C, class S, bool kInv = true>
+GLC_HD C dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start, const Tolerance& tol,
+                     C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite) {
   using namespace dp;
   C y0c[6];
 #pragma unroll
@@ -69,11 +75,22 @@ GLC_HD void dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], 
     inc[c] = h * (C(b1) * k1[c] + C(b3) * k3[c] + C(b4) * k4[c] + C(b5) * k5[c] + C(b6) * k6[c]);
     ys[c] = y0c[c] + inc[c];
   }
-  kn_rhs(k, ys, E, k7, r_end, vr_end);
+  kn_rhs<C, kInv>(k, ys, E, k7, r_end, vr_end, &inv);
   dt = h * (C(b1) * k1[6] + C(b3) * k3[6] + C(b4) * k4[6] + C(b5) * k5[6] + C(b6) * k6[6]);
+  C en = C(0), chk = dt + r_end;
+  if (kInv) chk += inv.lz + inv.carter;
 #pragma unroll
-  for (int c = 0; c < 7; ++c)
-    err[c] = h * (C(e1) * k1[c] + C(e3) * k3[c] + C(e4) * k4[c] + C(e5) * k5[c] + C(e6) * k6[c] + C(e7) * k7[c]);
+  for (int c = 0; c < 7; ++c) {
+    const C err = h * (C(e1) * k1[c] + C(e3) * k3[c] + C(e4) * k4[c] + C(e5) * k5[c] + C(e6) * k6[c] + C(e7) * k7[c]);
+    const C sv = c < 6 ? y0c[c] : t_start;
+    const C ev = c < 6 ? ys[c] : t_start + dt;
+    const bool pos = c < 3 || c == 6;
+    const C scale = C(pos ? tol.pos_rtol : tol.mom_rtol) * g_max(g_abs(sv), g_abs(ev)) + C(pos ? tol.pos_atol : tol.mom_atol);
+    en = g_max(en, g_abs(err) * g_rcp(scale));
+    chk += err + k7[c];
+  }
+  finite = g_finite(chk);
+  return en;
 }
 
 // Full stage set for dense output (the rare event path). K[0] must hold k1 on entry. The last

@@ -44,7 +44,7 @@ GLC_HD double g_rsqrt(double x) {
 }
 GLC_HD float g_rcp(float x) {
 #if defined(__CUDA_ARCH__)
-  return __frcp_rn(x);
+  return __fdividef(1.0f, x);
 #else
   return 1.0f / x;
 #endif
@@ -161,7 +161,14 @@ GLC_HD T kn_radius(const KN<T>& k, T x, T y, T z, int& status) {
 // Also returns r and the radial velocity dr/dlambda = grad(r) . x'. Non-finite values propagate
 // as NaN into the step's error norm, which the stepper turns into a numerical failure.
 template <class T>
-GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_out) {
+struct Invariants {
+  T lz, carter, null_residual;
+};
+
+// kInv: also evaluate L_z, Carter's constant and the normalized null residual at this point from
+// the same geometry (used on the end-of-step evaluation, whose point is the committed state).
+template <class T, bool kInv = false>
+GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_out, Invariants<T>* inv = nullptr) {
   const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
   const T R2 = x * x + yy * yy + z * z;
   const T b = R2 - k.a2;
@@ -213,6 +220,23 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
   d[6] = E + fq;
   r_out = r;
   vr_out = grx * vx + gry * vy + grz * vz;
+  if (kInv) {
+    // Carter's constant in the axis-regular Cartesian form (see kn_invariants)
+    const T rho2 = x * x + yy * yy;
+    const T Sxy = x * px + yy * py;
+    const T pp2 = px * px + py * py;
+    inv->lz = x * py - yy * px;
+    inv->carter = z * z * inv_r2 * (A * pp2 - k.a2 * E * E) - T(2) * z * Sxy * pz + r2 * rho2 * inv_A * pz * pz;
+    // g^{mu nu} p_mu p_nu with m = eta - f l l and u_i = l^i p_i (u_0 = E): diagonal terms
+    // eta_ii p_i^2 - f u_i^2, off-diagonal -f u_i u_j
+    const T u1 = lx * px, u2 = ly * py, u3 = lz * pz;
+    const T sum = -E * E + pp2 + pz * pz - f * q * q;
+    const T au = g_abs(E) + g_abs(u1) + g_abs(u2) + g_abs(u3);
+    const T su2 = E * E + u1 * u1 + u2 * u2 + u3 * u3;
+    const T norm = E * E * g_abs(T(1) + f) + g_abs(px * px - f * u1 * u1) + g_abs(py * py - f * u2 * u2) +
+                   g_abs(pz * pz - f * u3 * u3) + g_abs(f) * (au * au - su2);
+    inv->null_residual = norm > T(0) ? g_abs(sum) * g_rcp(norm) * g_min(norm, T(1)) : T(0);
+  }
 }
 
 // Conserved quantities and the normalized null residual (the reference's drift diagnostics,
@@ -221,11 +245,6 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
 //   Q = (z^2 / r^2) (A P_perp^2 - a^2 E^2) - 2 z S p_z + (r^2 rho^2 / A) p_z^2,
 //   S = x p_x + y p_y, P_perp^2 = p_x^2 + p_y^2, rho^2 = x^2 + y^2,
 // which equals the oracle's trigonometric form p_theta^2 + cos^2(theta)(L_z^2/sin^2 - a^2 E^2).
-template <class T>
-struct Invariants {
-  T lz, carter, null_residual;
-};
-
 template <class T>
 GLC_HD Invariants<T> kn_invariants(const KN<T>& k, const T y[6], T E, T r) {
   const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
@@ -258,6 +277,49 @@ GLC_HD Invariants<T> kn_invariants(const KN<T>& k, const T y[6], T E, T r) {
   // (numerics.rs:3-35) with its overflow-safe product collapsed for finite moderate inputs.
   out.null_residual = norm > T(0) ? g_abs(sum) / norm * g_min(norm, T(1)) : T(0);
   return out;
+}
+
+// Binary64 reciprocal from a binary32 seed and one Newton step (relative error ~1e-14): the
+// MIXED path's binary64 quantities without binary64 division sequences.
+GLC_HD double rcp_refined(double x) {
+  const double r0 = double(g_rcp(float(x)));
+  return r0 * (2.0 - x * r0);
+}
+
+// Binary64 invariants at a binary64 state, with r seeded by the binary32 right-hand side at the
+// same point (r_hint) and refined by Newton steps on r^4 - b r^2 - a^2 z^2 = 0.
+GLC_HD Invariants<double> kn_invariants_mixed(const KN<double>& k, const double y[6], double E, float r_hint) {
+  const double x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
+  const double b = x * x + yy * yy + z * z - k.a2;
+  const double az2 = k.a2 * z * z;
+  double u = double(r_hint) * double(r_hint);
+  u -= (u * u - b * u - az2) * rcp_refined(2.0 * u - b);
+  u -= (u * u - b * u - az2) * rcp_refined(2.0 * u - b);
+  const double rh = double(r_hint);
+  const double r = rh + (u - rh * rh) * (0.5 * rcp_refined(rh));
+  const double inv_r2 = rcp_refined(u);
+  const double inv_r = r * inv_r2;
+  const double A = u + k.a2;
+  const double inv_A = rcp_refined(A);
+  const double rho2 = x * x + yy * yy;
+  const double Sxy = x * px + yy * py;
+  const double pp2 = px * px + py * py;
+  Invariants<double> inv;
+  inv.lz = x * py - yy * px;
+  inv.carter = z * z * inv_r2 * (A * pp2 - k.a2 * E * E) - 2.0 * z * Sxy * pz + u * rho2 * inv_A * pz * pz;
+  const double f = (2.0 * r - k.q2) * rcp_refined(u + az2 * inv_r2);
+  const double lx = k.s * (r * x + k.sa * yy) * inv_A;
+  const double ly = k.s * (r * yy - k.sa * x) * inv_A;
+  const double lz = k.s * z * inv_r;
+  const double q = E + lx * px + ly * py + lz * pz;
+  const double u1 = lx * px, u2 = ly * py, u3 = lz * pz;
+  const double sum = -E * E + pp2 + pz * pz - f * q * q;
+  const double au = fabs(E) + fabs(u1) + fabs(u2) + fabs(u3);
+  const double su2 = E * E + u1 * u1 + u2 * u2 + u3 * u3;
+  const double norm = E * E * fabs(1.0 + f) + fabs(px * px - f * u1 * u1) + fabs(py * py - f * u2 * u2) +
+                      fabs(pz * pz - f * u3 * u3) + fabs(f) * (au * au - su2);
+  inv.null_residual = norm > 0.0 ? fabs(sum) * rcp_refined(norm) * (norm < 1.0 ? norm : 1.0) : 0.0;
+  return inv;
 }
 
 }  // namespace glc

@@ -110,12 +110,13 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
   if (o.event) reinterpret_cast<double2*>(o.event)[slot] = make_double2(double(res.event_residual), double(ray.affine));
   if (o.drift_a) reinterpret_cast<double2*>(o.drift_a)[slot] = make_double2(double(ray.dnull), 0.0);
   if (o.drift_b) reinterpret_cast<double2*>(o.drift_b)[slot] = make_double2(double(ray.dlz), double(ray.dq));
-  if (o.turning) reinterpret_cast<double2*>(o.turning)[slot] = make_double2(double(ray.turn_r), double(ray.az_adv));
-  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = make_double2(double(res.y[0]), double(res.y[1]));
+  if (o.turning)
+    reinterpret_cast<double2*>(o.turning)[slot] = make_double2(double(ray.turn_r), double(ray.azimuth_advance()));
+  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = make_double2(double(ray.y[0]), double(ray.y[1]));
   if (o.position_zr) {
     int gs;
-    const double r = kn_radius(ls.kn, double(res.y[0]), double(res.y[1]), double(res.y[2]), gs);
-    reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(res.y[2]), r);
+    const double r = kn_radius(ls.kn, double(ray.y[0]), double(ray.y[1]), double(ray.y[2]), gs);
+    reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(ray.y[2]), r);
   }
 }
 

@@ -145,7 +145,6 @@ template <class S>
 struct RayResult {
   uint32_t termination, failure, candidates, flags;
   S event_residual;
-  S y[6];
   S escape_theta, escape_phi;
   S surface_r, surface_phi, g;
 };
@@ -243,7 +242,21 @@ GLC_HD bool renormalize_null(const KN<T>& k, T y[6], T E) {
   return true;
 }
 
+template <int P>
+struct Ray;
+
+#if defined(__CUDA_ARCH__)
+template <int P>
+__device__ __noinline__ bool rare_step_outline(Ray<P>& ray, const LaneScene& sc, const glc_policy& pol,
+                                               RayResult<typename PrecTraits<P>::S>& res,
+                                               typename PrecTraits<P>::C en) {
+  return ray.rare_step(sc, pol, res, en, false);
+}
+#endif
+
 // ----------------------------------------------------------------------------------------------
+// One ray's trace state. S holds the state accumulators; bookkeeping that needs no more than the
+// stepping precision (step size, event values, drifts) is kept in C.
 template <int P>
 struct Ray {
   using S = typename PrecTraits<P>::S;
@@ -251,32 +264,31 @@ struct Ray {
 
   S y[6];
   S E;
-  S h;
   S affine;
   S tsum, tcorr;
-  S k1[7];
-  S r, vr;
-  S lz0, q0, dnull, dlz, dq;
-  S az_prev, az_adv;
-  S turn_r;
-  S dir;
+  S az0;          // initial azimuth; the advance is az_end - az0 + 2 pi * winding
+  C h;
+  C k1[7];        // FSAL derivative at y (precision C; MIXED recomputes it in double on shell steps)
+  S r, vr;        // event-function inputs at y: the exact values the previous step's checks used
+                  // (storage precision, so a binary64 re-check's sign survives being stored)
+  C lz0, q0, dnull, dlz, dq;
+  C turn_r;
+  C dir;
   uint32_t accepted, rejected, f64steps, consecutive;
   uint32_t armed;
-  uint32_t k1_f64;
   uint32_t turnings, crossings;
   int32_t winding, polar;
   uint32_t flags;
   bool have_inv;
 
-  // Initial state: y (position, covariant spatial momentum) and energy E = -p_t.
   GLC_HD void init(const LaneScene& sc, const glc_policy& pol, const double st8[8], double direction) {
     for (int c = 0; c < 3; ++c) {
       y[c] = S(st8[1 + c]);
       y[3 + c] = S(st8[5 + c]);
     }
     E = S(-st8[4]);
-    dir = S(direction);
-    h = dir * S(pol.initial_step);
+    dir = C(direction);
+    h = dir * C(pol.initial_step);
     affine = S(0);
     tsum = S(0);
     tcorr = S(0);
@@ -285,92 +297,65 @@ struct Ray {
     winding = 0;
     flags = 0;
     polar = st8[3] > 0.0 ? 1 : (st8[3] < 0.0 ? -1 : 0);
-    turn_r = S(NAN);
-    az_prev = g_atan2(y[1], y[0]);
-    az_adv = S(0);
-    dnull = dlz = dq = S(0);
-    const KN<S> ks = kn_cast<S>(sc.kn);
-    int gs;
-    const S r0 = kn_radius(ks, y[0], y[1], y[2], gs);
-    // initial invariants (geodesic.rs:101) and arming (geodesic.rs:536-544)
-    have_inv = gs == kGeomOk;
+    turn_r = C(NAN);
+    az0 = g_atan2(y[1], y[0]);
+    dnull = dlz = dq = C(0);
+    // first derivative (FSAL seed), the invariants at the start and the event arming
+    // (geodesic.rs:98-136, 536-544)
+    const KN<C> kc = kn_cast<C>(sc.kn);
+    C yc[6], rr, vv;
+    Invariants<C> inv;
+    for (int c = 0; c < 6; ++c) yc[c] = C(y[c]);
+    kn_rhs<C, true>(kc, yc, C(E), k1, rr, vv, &inv);
+    r = S(rr);
+    vr = S(vv);
+    have_inv = g_finite(rr) && g_finite(inv.lz) && g_finite(inv.carter) && g_finite(inv.null_residual);
+    lz0 = inv.lz;
+    q0 = inv.carter;
     armed = 0;
     if (have_inv) {
-      const Invariants<S> inv = kn_invariants(ks, y, E, r0);
-      lz0 = inv.lz;
-      q0 = inv.carter;
-      have_inv = g_finite(inv.lz) && g_finite(inv.carter) && g_finite(inv.null_residual);
+      dnull = inv.null_residual;
       for (int kind = 0; kind < 4; ++kind) {
-        const S v = event_value<S>(kind, sc, pol.singularity_guard, r0, y[2]);
+        const S v = event_value<S>(kind, sc, pol.singularity_guard, r, y[2]);
         if (event_clears_band(kind, v, S(pol.event_arming_band))) armed |= 1u << kind;
       }
     }
-    // first derivative (FSAL seed)
-    const KN<C> kc = kn_cast<C>(sc.kn);
-    C yc[6], d[7], rr, vv;
-    for (int c = 0; c < 6; ++c) yc[c] = C(y[c]);
-    kn_rhs(kc, yc, C(E), d, rr, vv);
-    for (int c = 0; c < 7; ++c) k1[c] = S(d[c]);
-    r = S(rr);
-    vr = S(vv);
-    k1_f64 = (P == kFP64) ? 1u : 0u;
-    if (have_inv) update_invariants(sc, y, r0);
   }
 
-  GLC_HD void update_invariants(const LaneScene& sc, const S yy[6], S rr) {
+  template <class T>
+  GLC_HD void update_drifts(const Invariants<T>& inv) {
     if (!have_inv) return;
-    const Invariants<S> inv = kn_invariants(kn_cast<S>(sc.kn), yy, E, rr);
-    if (g_finite(inv.null_residual)) dnull = g_max(dnull, inv.null_residual);
-    if (g_finite(inv.lz)) dlz = g_max(dlz, g_abs(inv.lz - lz0) / g_max(g_abs(lz0), S(1)));
-    if (g_finite(inv.carter)) dq = g_max(dq, g_abs(inv.carter - q0) / g_max(g_abs(q0), S(1)));
+    if (g_finite(inv.null_residual)) dnull = g_max(dnull, C(inv.null_residual));
+    if (g_finite(inv.lz)) dlz = g_max(dlz, C(g_abs(T(inv.lz) - T(lz0)) / g_max(g_abs(T(lz0)), T(1))));
+    if (g_finite(inv.carter)) dq = g_max(dq, C(g_abs(T(inv.carter) - T(q0)) / g_max(g_abs(T(q0)), T(1))));
   }
 
-  GLC_HD S next_step(const glc_policy& pol, S mag, S en, bool accepted_step) const {
-    const S maxf = accepted_step ? S(pol.maximum_factor) : S(1);
-    S factor;
-    if (en == S(0)) {
+  GLC_HD C next_step(const glc_policy& pol, C mag, C en, bool accepted_step) const {
+    const C maxf = accepted_step ? C(pol.maximum_factor) : C(1);
+    C factor;
+    if (en == C(0)) {
       factor = maxf;
     } else {
-      factor = S(pol.safety) * g_pow_m02(en);
-      factor = factor < S(pol.minimum_factor) ? S(pol.minimum_factor) : (factor > maxf ? maxf : factor);
+      factor = C(pol.safety) * g_pow_m02(en);
+      factor = factor < C(pol.minimum_factor) ? C(pol.minimum_factor) : (factor > maxf ? maxf : factor);
     }
-    S hn = mag * factor;
-    hn = hn < S(pol.minimum_step) ? S(pol.minimum_step) : (hn > S(pol.maximum_step) ? S(pol.maximum_step) : hn);
+    C hn = mag * factor;
+    hn = hn < C(pol.minimum_step) ? C(pol.minimum_step) : (hn > C(pol.maximum_step) ? C(pol.maximum_step) : hn);
     return hn;
   }
 
-  GLC_HD void commit_azimuth(const S yy[6]) {
-    const S az = g_atan2(yy[1], yy[0]);
-    const S raw = az - az_prev;
+  // Winding of the azimuth about the z axis (geodesic.rs:406-418): a wrap of atan2(y, x) happens
+  // only when y changes sign, so the azimuths are evaluated on those steps alone.
+  GLC_HD void commit_azimuth(const S y_old[6], const S y_new[6]) {
+    if (g_signbit(y_old[1]) == g_signbit(y_new[1])) return;
+    const S raw = g_atan2(y_new[1], y_new[0]) - g_atan2(y_old[1], y_old[0]);
     const S pi = S(3.14159265358979323846);
-    az_adv += wrapped_angle(az, az_prev);
     if (raw > pi) winding -= 1;
     else if (raw < -pi) winding += 1;
-    az_prev = az;
   }
 
-  // Compute one attempt in precision CC; results are returned in S.
-  template <class CC>
-  GLC_HD void attempt(const LaneScene& sc, S inc[6], S& dt, S err[7], S k7[7], S& r_end, S& vr_end, bool recompute_k1) {
-    const KN<CC> kc = kn_cast<CC>(sc.kn);
-    CC k1c[7];
-    if (recompute_k1) {
-      CC yc[6], rr, vv;
-      for (int c = 0; c < 6; ++c) yc[c] = CC(y[c]);
-      kn_rhs(kc, yc, CC(E), k1c, rr, vv);
-    } else {
-      for (int c = 0; c < 7; ++c) k1c[c] = CC(k1[c]);
-    }
-    CC incc[6], dtc, errc[7], k7c[7], rc, vc;
-    dp5_attempt<CC, S>(kc, y, CC(E), CC(h), k1c, incc, dtc, errc, k7c, rc, vc);
-    for (int c = 0; c < 6; ++c) inc[c] = S(incc[c]);
-    for (int c = 0; c < 7; ++c) {
-      err[c] = S(errc[c]);
-      k7[c] = S(k7c[c]);
-    }
-    dt = S(dtc);
-    r_end = S(rc);
-    vr_end = S(vc);
+  GLC_HD S azimuth_advance() const {
+    return g_atan2(y[1], y[0]) - az0 + S(6.28318530717958647692) * S(winding);
   }
 
   // Advance by one attempted step. Returns true when the ray terminated (result filled).
@@ -380,47 +365,57 @@ struct Ray {
       finish_plain(res, GLC_TERM_STEP_EXHAUSTION, GLC_FAIL_NONE);
       return true;
     }
-    S inc[6], dt, err[7], k7[7], r_end, vr_end;
-    bool stepped64 = false;
-    if (P == kMIXED && kUse64) {
-      attempt<double>(sc, inc, dt, err, k7, r_end, vr_end, k1_f64 == 0u);
-      stepped64 = true;
-    } else {
-      attempt<C>(sc, inc, dt, err, k7, r_end, vr_end, false);
-    }
-    // grouped infinity norm with the relative coordinate time (geodesic.rs:158-165)
-    const S t_start = tsum + tcorr;
-    S en = S(0);
-    bool finite = g_finite(dt) && g_finite(r_end);
-    for (int c = 0; c < 7; ++c) {
-      S sc_, ec;
-      if (c < 6) {
-        sc_ = y[c];
-        ec = y[c] + inc[c];
-      } else {
-        sc_ = t_start;
-        ec = t_start + dt;
+    const Tolerance tol{pol.position_rtol, pol.position_atol, pol.momentum_rtol, pol.momentum_atol};
+    S inc[6], r_end, vr_end;
+    C dt, k7[7], en;
+    Invariants<C> inv;
+    bool finite;
+    const bool stepped64 = P == kMIXED && kUse64;
+    if (stepped64) {
+      // binary64 step inside the shell: double k1 at y, double stages and error control
+      const KN<double> kd = sc.kn;
+      double yd[6], k1d[7], rr, vv, incd[6], dtd, k7d[7], red, vred;
+      Invariants<double> invd;
+      for (int c = 0; c < 6; ++c) yd[c] = double(y[c]);
+      kn_rhs(kd, yd, double(E), k1d, rr, vv);
+      const double end = dp5_attempt<double, double>(kd, yd, double(E), double(h), k1d, double(tsum + tcorr), tol,
+                                                     incd, dtd, k7d, red, vred, invd, finite);
+      for (int c = 0; c < 6; ++c) inc[c] = S(incd[c]);
+      for (int c = 0; c < 7; ++c) k7[c] = C(k7d[c]);
+      dt = C(dtd);
+      r_end = S(red);
+      vr_end = S(vred);
+      inv.lz = C(invd.lz);
+      inv.carter = C(invd.carter);
+      inv.null_residual = C(invd.null_residual);
+      en = C(end);
+      if (finite && end <= 1.0) {
+        // drifts from the binary64 evaluation
+        update_drifts(invd);
+        inv.null_residual = C(NAN);  // already folded in
       }
-      const bool pos = (c < 3) || (c == 6);
-      const S rtol = pos ? S(pol.position_rtol) : S(pol.momentum_rtol);
-      const S atol = pos ? S(pol.position_atol) : S(pol.momentum_atol);
-      const S scale = rtol * g_max(g_abs(sc_), g_abs(ec)) + atol;
-      const S q = g_abs(err[c]) / scale;
-      finite = finite && g_finite(err[c]) && g_finite(inc[c > 5 ? 5 : c]);
-      en = g_max(en, q);
+    } else {
+      const KN<C> kc = kn_cast<C>(sc.kn);
+      C incc[6], rec, vrec;
+      // MIXED evaluates the invariants in binary64 at the committed state instead
+      en = dp5_attempt<C, S, P != kMIXED>(kc, y, C(E), h, k1, C(tsum + tcorr), tol, incc, dt, k7, rec, vrec,
+                                          inv, finite);
+      for (int c = 0; c < 6; ++c) inc[c] = S(incc[c]);
+      r_end = S(rec);
+      vr_end = S(vrec);
     }
     if (!finite || !g_finite(en)) {
       finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
       return true;
     }
-    if (en > S(1)) {
+    if (en > C(1)) {
       rejected += 1;
       consecutive += 1;
       if (consecutive >= pol.maximum_consecutive_rejects) {
         finish_plain(res, GLC_TERM_REJECT_EXHAUSTION, GLC_FAIL_NONE);
         return true;
       }
-      if (g_abs(h) <= S(pol.minimum_step)) {
+      if (g_abs(h) <= C(pol.minimum_step)) {
         finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_MINIMUM_STEP);
         return true;
       }
@@ -435,34 +430,44 @@ struct Ray {
     }
     S yend[6];
     for (int c = 0; c < 6; ++c) yend[c] = y[c] + inc[c];
-    // ---- crossing detection at both ends (values from the FSAL evaluations)
+    // ---- crossing detection: start values are exactly the previous step's end values
     const double guard = pol.singularity_guard;
-    uint32_t ev_mask = 0;
+    bool any = false;
     for (int kind = 0; kind < 4; ++kind) {
       if (!((armed >> kind) & 1u) || !((sc.installed >> kind) & 1u)) continue;
       const S sv = event_value<S>(kind, sc, guard, r, y[2]);
       const S evv = event_value<S>(kind, sc, guard, r_end, yend[2]);
-      if (event_crosses(kind, sv, evv)) ev_mask |= 1u << kind;
+      any = any || event_crosses(kind, sv, evv);
     }
-    const S vs = dir * vr, ve = dir * vr_end;
-    const bool turning = (vs < S(0) && ve >= S(0)) || (vs > S(0) && ve <= S(0));
-    const bool equator = event_crosses(kEvSurface, y[2], yend[2]);
-    if (ev_mask != 0u || turning || equator) {
-      return rare_step(sc, pol, res, en);
+    const S vs = S(dir) * vr, ve = S(dir) * vr_end;
+    any = any || (vs < S(0) && ve >= S(0)) || (vs > S(0) && ve <= S(0));
+    any = any || event_crosses(kEvSurface, y[2], yend[2]);
+    if (any) {
+#if defined(__CUDA_ARCH__)
+      // out-of-line event path on copies, so the hot loop keeps this ray in registers
+      Ray tmp = *this;
+      LaneScene lsc = sc;
+      glc_policy pl = pol;
+      RayResult<S> rs;
+      const bool done = rare_step_outline<P>(tmp, lsc, pl, rs, en);
+      *this = tmp;
+      if (done) res = rs;
+      return done;
+#else
+      return rare_step(sc, pol, res, en, stepped64);
+#endif
     }
     // ---- plain commit
-    CompSum::add(tsum, tcorr, dt);
-    commit_azimuth(yend);
-    S rc = r_end;
-    if (P == kMIXED) {
-      int gs;
-      rc = kn_radius(kn_cast<S>(sc.kn), yend[0], yend[1], yend[2], gs);
+    CompSum::add(tsum, tcorr, S(dt));
+    commit_azimuth(y, yend);
+    if constexpr (P == kMIXED) {
+      if (!stepped64) update_drifts(kn_invariants_mixed(sc.kn, yend, double(E), float(r_end)));
+    } else {
+      update_drifts(inv);
     }
-    update_invariants(sc, yend, rc);
-    affine += h;
+    affine += S(h);
     for (int c = 0; c < 6; ++c) y[c] = yend[c];
     for (int c = 0; c < 7; ++c) k1[c] = k7[c];
-    k1_f64 = (P == kFP64 || stepped64) ? 1u : 0u;
     r = r_end;
     vr = vr_end;
     arm_update(sc, pol);
@@ -479,27 +484,29 @@ struct Ray {
     }
   }
 
-  // Event path in S precision: recompute the stages for dense output, localize, commit.
-  GLC_HD bool rare_step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, S en) {
+  // Event path in precision S (binary64 in MIXED): recompute the stages for dense output, then
+  // localize events, turning points and equatorial crossings and commit. The sign tests use the
+  // stored start values (r, vr: what the previous step's end checks used), so a crossing is never
+  // lost between a binary32 detection and a binary64 re-check.
+  GLC_HD bool rare_step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, C en, bool stepped64) {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
     T K[7][7];
-    T r0 = r, vr0 = vr;
-    if (P == kMIXED && k1_f64 == 0u) {
+    {
       T rr, vv;
-      kn_rhs(kt, y, E, K[0], rr, vv);
-      r0 = rr;
-      vr0 = vv;
-    } else {
-      for (int c = 0; c < 7; ++c) K[0][c] = k1[c];
+      if (P == kMIXED) {
+        kn_rhs(kt, y, E, K[0], rr, vv);
+      } else {
+        for (int c = 0; c < 7; ++c) K[0][c] = T(k1[c]);
+      }
     }
-    const T hh = h;
+    const T r0 = T(r), vr0 = T(vr);
+    const T hh = T(h);
     T yend[6], r_end, vr_end;
     dp5_stages(kt, y, E, hh, K, yend, r_end, vr_end);
     const double guard = pol.singularity_guard;
     const T tol = T(pol.event_affine_tolerance);
     bool fail = false;
-    // events in the reference order: guard, horizon, surface, escape
     int n = 0;
     int kinds[4];
     T thetas[4], residuals[4], states[4][6];
@@ -510,9 +517,9 @@ struct Ray {
       if (!event_crosses(kind, sv, evv)) continue;
       T th, yr[6], br;
       auto value_at = [&](const T* ys, T& v) -> bool {
-        int gs;
+        int gs = kGeomOk;
         const T rr = kind == kEvSurface ? T(0) : kn_radius(kt, ys[0], ys[1], ys[2], gs);
-        if (kind != kEvSurface && gs != kGeomOk) return false;
+        if (gs != kGeomOk) return false;
         v = event_value<T>(kind, sc, guard, rr, ys[2]);
         return true;
       };
@@ -554,13 +561,13 @@ struct Ray {
     const T term_theta = has_event ? thetas[first] : T(1);
     // radial turning point (geodesic.rs:330-360)
     {
-      const T sv = dir * vr0, evv = dir * vr_end;
+      const T sv = T(dir) * vr0, evv = T(dir) * vr_end;
       if ((sv < T(0) && evv >= T(0)) || (sv > T(0) && evv <= T(0))) {
         T th, yr[6], br;
         auto vr_at = [&](const T* ys, T& v) -> bool {
           T d[7], rr, vv;
           kn_rhs(kt, ys, E, d, rr, vv);
-          v = dir * vv;
+          v = T(dir) * vv;
           return g_finite(v);
         };
         if (localize(y, hh, K, tol, sv, evv, vr_at, th, yr, br) && (!has_event || th < term_theta)) {
@@ -568,7 +575,7 @@ struct Ray {
           if (sv < T(0) && evv >= T(0)) {
             int gs;
             const T rr = kn_radius(kt, yr[0], yr[1], yr[2], gs);
-            if (gs == kGeomOk) turn_r = (turn_r == turn_r) ? g_min(turn_r, rr) : rr;
+            if (gs == kGeomOk) turn_r = (turn_r == turn_r) ? C(g_min(T(turn_r), rr)) : C(rr);
           }
         }
       }
@@ -584,39 +591,37 @@ struct Ray {
     }
     // commit at the terminal theta (or the step end)
     T ycommit[6], dtc;
-    if (has_event) {
+    {
       T ytmp[6];
       dense_eval(y, hh, K, term_theta, ytmp, dtc);
-      for (int c = 0; c < 6; ++c) ycommit[c] = states[first][c];
-    } else {
-      dense_eval(y, hh, K, T(1), ycommit, dtc);
-      for (int c = 0; c < 6; ++c) ycommit[c] = yend[c];
+      for (int c = 0; c < 6; ++c) ycommit[c] = has_event ? states[first][c] : yend[c];
     }
     CompSum::add(tsum, tcorr, dtc);
-    commit_azimuth(ycommit);
+    commit_azimuth(y, ycommit);
     {
       int gs;
       const T rr = kn_radius(kt, ycommit[0], ycommit[1], ycommit[2], gs);
-      if (gs == kGeomOk) update_invariants(sc, ycommit, rr);
+      if (gs == kGeomOk) update_drifts(kn_invariants(kt, ycommit, E, rr));
     }
     if (has_event) {
       affine = hh * term_theta + affine;
+      for (int c = 0; c < 6; ++c) y[c] = ycommit[c];
       const int kind = kinds[first];
       uint32_t term = GLC_TERM_HORIZON;
       if (kind == kEvGuard) term = GLC_TERM_SINGULARITY;
       else if (kind == kEvSurface) term = GLC_TERM_SURFACE;
       else if (kind == kEvEscape) term = GLC_TERM_ESCAPE;
-      finish_event(sc, pol, res, term, cand, residuals[first], ycommit);
+      finish_event(sc, pol, res, term, cand, residuals[first]);
       return true;
     }
     affine += hh;
     for (int c = 0; c < 6; ++c) y[c] = yend[c];
-    for (int c = 0; c < 7; ++c) k1[c] = K[6][c];
-    k1_f64 = (P == kFP32) ? 0u : 1u;
+    for (int c = 0; c < 7; ++c) k1[c] = C(K[6][c]);
     r = r_end;
     vr = vr_end;
     arm_update(sc, pol);
     h = dir * next_step(pol, g_abs(h), en, true);
+    (void)stepped64;
     return false;
   }
 
@@ -626,15 +631,17 @@ struct Ray {
     res.candidates = 0;
     res.flags = flags;
     res.event_residual = S(NAN);
-    for (int c = 0; c < 6; ++c) res.y[c] = y[c];
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
   }
 
+  // Terminal observables at the committed event state y (precision S; binary64 in MIXED).
   GLC_HD void finish_event(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, uint32_t term,
-                           uint32_t cand, S residual, S ye[6]) {
+                           uint32_t cand, S residual) {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
+    T ye[6];
+    for (int c = 0; c < 6; ++c) ye[c] = y[c];
     if (P == kMIXED && pol.renormalize_null) {
       if (renormalize_null(kt, ye, E)) flags |= kFlagRenormalized;
     }
@@ -642,13 +649,12 @@ struct Ray {
     res.failure = GLC_FAIL_NONE;
     res.candidates = cand;
     res.event_residual = residual;
-    for (int c = 0; c < 6; ++c) res.y[c] = ye[c];
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
     if (term == GLC_TERM_ESCAPE) {
       T d[7], rr, vv;
       kn_rhs(kt, ye, E, d, rr, vv);
-      const T dx = dir * d[0], dy = dir * d[1], dz = dir * d[2];
+      const T dx = T(dir) * d[0], dy = T(dir) * d[1], dz = T(dir) * d[2];
       const T nrm = g_sqrt(dx * dx + dy * dy + dz * dz);
       if (nrm > T(0) && g_finite(nrm)) {
         T cz = dz / nrm;

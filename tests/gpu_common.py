@@ -55,7 +55,8 @@ def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
         d = np.stack([ref[esc, F["escape_dx"]], ref[esc, F["escape_dy"]], ref[esc, F["escape_dz"]]], axis=1)
         v = unit(gpu["escape_theta"][sel][esc], gpu["escape_phi"][sel][esc])
         rep["escape_direction_rad"] = float(np.max(np.arccos(np.clip(np.sum(d * v, axis=1), -1.0, 1.0))))
-    srf = same & (ot == G.Termination.EQUATORIAL_SURFACE)
+    # surface observables exist only for observation traces (oracle surface_status == 1)
+    srf = same & (ot == G.Termination.EQUATORIAL_SURFACE) & (ref[:, F["surface_status"]] == 1)
     if srf.any():
         g0 = ref[srf, F["frequency_ratio"]]
         rep["g_rel"] = float(np.max(np.abs(gpu["frequency_ratio"][sel][srf] - g0) / g0))

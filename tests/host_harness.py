@@ -1,0 +1,47 @@
+"""Builds and loads tests/native/host_trace.cpp: the device tracer's per-ray logic compiled for the
+host (test infrastructure; the product path is the CUDA kernel)."""
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+SRC = ROOT / "tests" / "native" / "host_trace.cpp"
+OUT = ROOT / "tests" / "native" / "_build" / "libhost_trace.so"
+DEPS = [SRC] + sorted((ROOT / "gravlume_b200" / "csrc").glob("*.cuh")) + [ROOT / "include" / "glc.h"]
+
+FIELDS = ["termination", "failure", "candidates", "flags", "accepted_steps", "rejected_steps",
+          "radial_turnings", "equatorial_crossings", "azimuth_winding", "escape_theta", "escape_phi",
+          "source_radius", "source_azimuth", "frequency_ratio", "travel_time", "event_residual",
+          "affine_parameter", "max_null_residual", "max_lz_drift", "max_carter_drift", "turning_radius",
+          "azimuth_advance", "x", "y", "z", "p_x", "p_y", "p_z", "f64_steps"]
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not OUT.exists() or any(d.stat().st_mtime > OUT.stat().st_mtime for d in DEPS):
+            OUT.parent.mkdir(parents=True, exist_ok=True)
+            subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-x", "c++", str(SRC), "-o", str(OUT)],
+                           check=True)
+        L = ctypes.CDLL(str(OUT))
+        L.host_trace_states.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                        ctypes.c_double, ctypes.c_void_p]
+        assert L.host_trace_fields() == len(FIELDS)
+        _lib = L
+    return _lib
+
+
+def trace_states(scene, policy, states, direction):
+    st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+    out = np.zeros((st.shape[0], len(FIELDS)))
+    rc = lib().host_trace_states(ctypes.byref(scene), ctypes.byref(policy), st.shape[0], st.ctypes.data,
+                                 direction, out.ctypes.data)
+    assert rc == 0
+    d = {k: out[:, i] for i, k in enumerate(FIELDS)}
+    d["termination"] = d["termination"].astype(int)
+    return d

@@ -181,3 +181,16 @@ def test_ray_list_matches_the_oracle_on_random_kerr_newman_rays(pipe):
     print("raylist fp64", rep)
     assert rep["class_mismatch"] == 0
     assert rep.get("travel_time", 0.0) <= FP64_BUDGET["travel_time"]
+
+
+@pytest.mark.parametrize("precision", [G.Precision.MIXED, G.Precision.FP32, G.Precision.FP64])
+def test_full_hd_frame_never_exhausts_steps(pipe, precision):
+    """Every ray of a 1920x1080 frame ends at an event: a crossing lost between a binary32
+    detection and a binary64 re-check would leave the ray stepping to the accepted-step cap."""
+    obs = config1_observation(width=1920, height=1080)
+    d = run_image(pipe, obs, precision)
+    hist = np.bincount(d["termination"], minlength=9)
+    assert hist[G.Termination.STEP_EXHAUSTION] == 0, hist
+    assert hist[G.Termination.NUMERICAL_FAILURE] == 0, hist
+    assert hist[0] == 0  # every pixel written
+    assert d["accepted_steps"].max() < 20000

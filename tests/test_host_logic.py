@@ -1,0 +1,87 @@
+"""The device tracer's per-ray state machine, compiled for the host by the test harness
+(tests/native/host_trace.cpp), against the binary64 oracle: event arming and localization,
+turning points, equatorial crossings, winding and drifts in all three precision modes. The same
+budgets hold for the CUDA kernels in tests/test_gpu_parity.py."""
+
+import numpy as np
+import pytest
+
+import gravlume_b200 as G
+import host_harness as H
+import oracle as O
+from gpu_common import F, compare, config1_observation, oracle_for
+
+BUDGETS = {
+    G.Precision.FP64: dict(escape_direction_rad=1e-7, travel_time=1e-6, max_null_residual=1e-9,
+                           max_lz_drift=1e-8, max_carter_drift=1e-8),
+    G.Precision.MIXED: dict(escape_direction_rad=1e-6, travel_time=1e-3, max_null_residual=1e-5,
+                            max_lz_drift=1e-4, max_carter_drift=1e-4),
+    G.Precision.FP32: dict(escape_direction_rad=2e-3, travel_time=5e-2),
+}
+
+
+@pytest.fixture(scope="module")
+def config1_rays():
+    obs = config1_observation()
+    osc, ev, sc = oracle_for(obs)
+    rng = np.random.default_rng(11)
+    px, py = rng.integers(0, 256, 64), rng.integers(0, 256, 64)
+    states, _, _, status = O.initial_rays(osc, px, py)
+    assert (status == 0).all()
+    ref = O.trace_states(1.0, 0.9, 0.3, 1, O.custom_policy(1e-10, 1e-12), ev, states, -1.0,
+                         threads=O.hardware_threads())
+    return sc, states, ref
+
+
+@pytest.mark.parametrize("precision", [G.Precision.FP64, G.Precision.MIXED, G.Precision.FP32])
+def test_kernel_logic_matches_the_oracle(config1_rays, precision):
+    sc, states, ref = config1_rays
+    d = H.trace_states(sc, G.ReferencePolicy.frame(precision), states, -1.0)
+    rep = compare(d, np.arange(len(states)), ref)
+    assert rep["class_mismatch"] == 0, rep
+    assert rep["radial_turnings_mismatch"] == 0 and rep["equatorial_crossings_mismatch"] == 0, rep
+    for k, tol in BUDGETS[precision].items():
+        assert rep[k] <= tol, (k, rep)
+
+
+def test_mixed_errors_are_below_plain_fp32(config1_rays):
+    sc, states, ref = config1_rays
+    m = compare(H.trace_states(sc, G.ReferencePolicy.frame(G.Precision.MIXED), states, -1.0), np.arange(64), ref)
+    f = compare(H.trace_states(sc, G.ReferencePolicy.frame(G.Precision.FP32), states, -1.0), np.arange(64), ref)
+    for k in ("escape_direction_rad", "travel_time", "max_null_residual", "max_lz_drift", "max_carter_drift"):
+        assert m[k] <= f[k], (k, m[k], f[k])
+
+
+def test_escape_is_never_lost_across_precisions():
+    """A ray leaving the escape sphere must terminate there in every mode (no step exhaustion)."""
+    obs = config1_observation(width=64, height=64)
+    osc, ev, sc = oracle_for(obs)
+    px, py = np.meshgrid(np.arange(0, 64, 4), np.arange(0, 64, 4))
+    states, _, _, _ = O.initial_rays(osc, px.ravel(), py.ravel())
+    for prec in G.Precision:
+        d = H.trace_states(sc, G.ReferencePolicy.frame(prec), states, -1.0)
+        assert (d["termination"] != G.Termination.STEP_EXHAUSTION).all()
+        esc = d["termination"] == G.Termination.ESCAPE
+        assert esc.any()
+        r = np.sqrt(d["x"] ** 2 + d["y"] ** 2 + d["z"] ** 2)
+        assert np.all(np.abs(r[esc] - 1000.0) < 1e-2)
+
+
+def test_geodesic_fixtures_through_the_kernel_logic(golden):
+    for fid, policy in [("schwarzschild-scatter-b6-v1", G.ReferencePolicy.regular_v1()),
+                        ("schwarzschild-scatter-near-critical-v1", G.ReferencePolicy.strict_v1()),
+                        ("schwarzschild-capture-near-critical-v1", G.ReferencePolicy.strict_v1())]:
+        fx = golden[fid]
+        esc = float(fx["events"].get("escape_radius_m", 0.0))
+        sc = G.Observation(spin=0.0, chart=G.KerrSchildChart.INGOING, observer_txyz=(0.0, 60.0, 0.0, 1.0),
+                           escape_radius=esc).pack()
+        st = [float(v) for v in fx["initial"]["position_txyz_m"]] + [float(v) for v in fx["initial"]["momentum_covariant"]]
+        d = H.trace_states(sc, policy, [st], 1.0)
+        exp, tol = fx["expected"], fx["tolerance"]
+        want = G.Termination.ESCAPE if exp["termination"] == "escape" else G.Termination.HORIZON_CROSSING
+        assert d["termination"][0] == want
+        assert abs(d["azimuth_advance"][0] - float(exp["azimuth_advance_rad"])) <= float(tol["azimuth_advance_abs_rad"])
+        if "turning_radius_m" in exp:
+            assert abs(d["turning_radius"][0] - float(exp["turning_radius_m"])) <= float(tol["turning_radius_abs_m"])
+        else:
+            assert np.isnan(d["turning_radius"][0])
