@@ -327,11 +327,17 @@ def run_gpu(args) -> None:
                                     "sample": f"{args.cpu_sample} seeded pixels of the {WIDTH}x{HEIGHT} frame, "
                                               "binary64 oracle rtol 1e-10 atol 1e-12"}
             comp[args.precision] = error_report(G, d, ref, idx)
-        for name, prec in (("fp32", G.Precision.FP32), ("fp64", G.Precision.FP64)):
+        shape = {k: policy[k] for k in ("persistent", "block_threads", "tile_w", "tile_h", "refill_interval",
+                                         "rays_per_grab")}
+        frame_tol = {k: policy[k] for k in ("position_rtol", "position_atol", "momentum_rtol", "momentum_atol",
+                                             "maximum_step")}
+        runs = (("fp32", G.Precision.FP32, {}), ("mixed", G.Precision.MIXED, {}),
+                ("fp64_frame_tolerance", G.Precision.FP64, frame_tol),
+                ("fp64_oracle_policy", G.Precision.FP64, {}))
+        for name, prec, extra in runs:
             if name == args.precision:
                 continue
-            pipe.set_policy(G.ReferencePolicy.frame(prec, **{k: policy[k] for k in (
-                "persistent", "block_threads", "tile_w", "tile_h", "refill_interval", "rays_per_grab")}))
+            pipe.set_policy(G.ReferencePolicy.frame(prec, **shape, **extra))
             pipe.trace([scene], [cam], results, stream=stream)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -340,11 +346,14 @@ def run_gpu(args) -> None:
             torch.cuda.synchronize()
             ms = a.elapsed_time(b)
             dd = results.numpy()
-            entry = {"mrays_per_s": rays / (ms / 1e3) / 1e6, "ms": ms}
+            entry = {"mrays_per_s": rays / (ms / 1e3) / 1e6, "ms": ms,
+                     "attempts_per_ray": float((dd["accepted_steps"] + dd["rejected_steps"]).mean()),
+                     "policy": {k: getattr(pipe.policy, k) for k in ("position_rtol", "maximum_step")}}
             if ref is not None:
                 entry["error_vs_oracle"] = error_report(G, dd, ref, idx)
             comp[name] = entry
         comp[args.precision] = {"mrays_per_s": value / world, "ms": total_ms / args.steps,
+                                "attempts_per_ray": float((d["accepted_steps"] + d["rejected_steps"]).mean()),
                                 "error_vs_oracle": comp.get(args.precision)}
         line["precision_study"] = comp
     print(json.dumps(line), flush=True)
@@ -360,6 +369,7 @@ def ctypes_sizeof_job() -> int:
 
 
 def main() -> None:
+    global WIDTH, HEIGHT
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -375,7 +385,6 @@ def main() -> None:
     ap.add_argument("--width", type=int, default=WIDTH, help="frame width (smaller frames for profiling)")
     ap.add_argument("--height", type=int, default=HEIGHT, help="frame height")
     args = ap.parse_args()
-    global WIDTH, HEIGHT
     WIDTH, HEIGHT = args.width, args.height
     if args.impl == "reference":
         run_reference(args)

@@ -310,8 +310,11 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
       p.position_rtol = p.momentum_rtol = 1.0e-10;
       p.position_atol = p.momentum_atol = 1.0e-12;
     } else {
+      // error-controlled steps: the 0.5 M cap of the binary64 presets only multiplies far-field
+      // steps (the binary32 controller is roundoff-limited well before it matters)
       p.position_rtol = p.momentum_rtol = 1.0e-6;
       p.position_atol = p.momentum_atol = 1.0e-8;
+      p.maximum_step = 1.0e3;
       if (precision == GLC_FP32) {
         p.event_affine_tolerance = 1.0e-6;
         p.event_tie_tolerance = 2.0e-6;

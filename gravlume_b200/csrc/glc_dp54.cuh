@@ -77,8 +77,11 @@ GLC_HD C dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t
   }
   kn_rhs<C, kInv>(k, ys, E, k7, r_end, vr_end, &inv);
   dt = h * (C(b1) * k1[6] + C(b3) * k3[6] + C(b4) * k4[6] + C(b5) * k5[6] + C(b6) * k6[6]);
-  C en = C(0), chk = dt + r_end;
+  C chk = dt + r_end;
   if (kInv) chk += inv.lz + inv.carter;
+  // max_c |err_c| / scale_c with a single reciprocal: keep the running maximum as a fraction
+  // (num, den) and compare fractions by cross-multiplication (all scales are positive)
+  C num = C(0), den = C(1);
 #pragma unroll
   for (int c = 0; c < 7; ++c) {
     const C err = h * (C(e1) * k1[c] + C(e3) * k3[c] + C(e4) * k4[c] + C(e5) * k5[c] + C(e6) * k6[c] + C(e7) * k7[c]);
@@ -86,11 +89,14 @@ GLC_HD C dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t
     const C ev = c < 6 ? ys[c] : t_start + dt;
     const bool pos = c < 3 || c == 6;
     const C scale = C(pos ? tol.pos_rtol : tol.mom_rtol) * g_max(g_abs(sv), g_abs(ev)) + C(pos ? tol.pos_atol : tol.mom_atol);
-    en = g_max(en, g_abs(err) * g_rcp(scale));
+    const C ae = g_abs(err);
+    const bool larger = ae * den > num * scale;
+    num = larger ? ae : num;
+    den = larger ? scale : den;
     chk += err + k7[c];
   }
   finite = g_finite(chk);
-  return en;
+  return num * g_rcp(den);
 }
 
 // Full stage set for dense output (the rare event path). K[0] must hold k1 on entry. The last
@@ -142,6 +148,22 @@ GLC_HD void dense_eval(const T y0[6], T h, const T K[7][7], T th, T y[6], T& dt)
     T s = T(0);
 #pragma unroll
     for (int j = 0; j < 7; ++j) s += w[j] * K[j][c];
+    if (c < 6) y[c] = y0[c] + h * s;
+    else dt = h * s;
+  }
+}
+
+// Dense output with stages in TK accumulated in T (binary64 dense state from binary32 stages in
+// the MIXED event path).
+template <class T, class TK>
+GLC_HD void dense_eval_mixed(const T y0[6], T h, const TK K[7][7], T th, T y[6], T& dt) {
+  T w[7];
+  dense_weights(th, w);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) s += w[j] * T(K[j][c]);
     if (c < 6) y[c] = y0[c] + h * s;
     else dt = h * s;
   }

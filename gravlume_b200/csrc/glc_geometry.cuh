@@ -184,9 +184,11 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
   const T r = r2 * inv_r;
   const T inv_r2 = inv_r * inv_r;
   const T A = r2 + k.a2;
-  const T inv_A = g_rcp(A);
   const T sigma = r2 + az2 * inv_r2;  // (r^4 + a^2 z^2) / r^2
-  const T inv_sigma = g_rcp(sigma);
+  // one reciprocal for both denominators: 1/A = sigma/(A sigma), 1/sigma = A/(A sigma)
+  const T inv_As = g_rcp(A * sigma);
+  const T inv_A = sigma * inv_As;
+  const T inv_sigma = A * inv_As;
   // grad r = (x r, y r, z A / r) / sigma
   const T rs = r * inv_sigma;
   const T grx = x * rs, gry = yy * rs, grz = z * A * inv_r * inv_sigma;
@@ -286,19 +288,16 @@ GLC_HD double rcp_refined(double x) {
   return r0 * (2.0 - x * r0);
 }
 
-// Binary64 invariants at a binary64 state, with r seeded by the binary32 right-hand side at the
-// same point (r_hint) and refined by Newton steps on r^4 - b r^2 - a^2 z^2 = 0.
+// Binary64 L_z and Carter's constant at a binary64 state, with r^2 seeded by the binary32
+// right-hand side at the same point (r_hint) and refined by one Newton step on
+// u^2 - b u - a^2 z^2 = 0 (u = r^2); null_residual is left at 0 for the caller to fill.
 GLC_HD Invariants<double> kn_invariants_mixed(const KN<double>& k, const double y[6], double E, float r_hint) {
   const double x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
   const double b = x * x + yy * yy + z * z - k.a2;
   const double az2 = k.a2 * z * z;
   double u = double(r_hint) * double(r_hint);
-  u -= (u * u - b * u - az2) * rcp_refined(2.0 * u - b);
-  u -= (u * u - b * u - az2) * rcp_refined(2.0 * u - b);
-  const double rh = double(r_hint);
-  const double r = rh + (u - rh * rh) * (0.5 * rcp_refined(rh));
+  u -= (u * u - b * u - az2) * double(g_rcp(float(2.0 * u - b)));
   const double inv_r2 = rcp_refined(u);
-  const double inv_r = r * inv_r2;
   const double A = u + k.a2;
   const double inv_A = rcp_refined(A);
   const double rho2 = x * x + yy * yy;
@@ -307,18 +306,7 @@ GLC_HD Invariants<double> kn_invariants_mixed(const KN<double>& k, const double 
   Invariants<double> inv;
   inv.lz = x * py - yy * px;
   inv.carter = z * z * inv_r2 * (A * pp2 - k.a2 * E * E) - 2.0 * z * Sxy * pz + u * rho2 * inv_A * pz * pz;
-  const double f = (2.0 * r - k.q2) * rcp_refined(u + az2 * inv_r2);
-  const double lx = k.s * (r * x + k.sa * yy) * inv_A;
-  const double ly = k.s * (r * yy - k.sa * x) * inv_A;
-  const double lz = k.s * z * inv_r;
-  const double q = E + lx * px + ly * py + lz * pz;
-  const double u1 = lx * px, u2 = ly * py, u3 = lz * pz;
-  const double sum = -E * E + pp2 + pz * pz - f * q * q;
-  const double au = fabs(E) + fabs(u1) + fabs(u2) + fabs(u3);
-  const double su2 = E * E + u1 * u1 + u2 * u2 + u3 * u3;
-  const double norm = E * E * fabs(1.0 + f) + fabs(px * px - f * u1 * u1) + fabs(py * py - f * u2 * u2) +
-                      fabs(pz * pz - f * u3 * u3) + fabs(f) * (au * au - su2);
-  inv.null_residual = norm > 0.0 ? fabs(sum) * rcp_refined(norm) * (norm < 1.0 ? norm : 1.0) : 0.0;
+  inv.null_residual = 0.0;
   return inv;
 }
 

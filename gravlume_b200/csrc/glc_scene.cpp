@@ -181,16 +181,20 @@ double det4(const double c0[4], const double c1[4], const double c2[4], const do
 }
 
 // Equatorial circular photon orbits of Kerr-Newman (M = 1): roots of
-//   r^2 - 3 r + 2 Q^2 +- 2 a sqrt(r - Q^2) = 0 ("-": retrograde, the outer one).
+//   r^2 - 3 r + 2 Q^2 + sign * 2 |a| sqrt(r - Q^2) = 0
+// (sign +1: prograde, the inner orbit; -1: retrograde, the outer one). The function is positive
+// above the orbit; walk down from 6 M to the first non-positive value and bisect.
 double photon_orbit(double a, double q, double sign) {
   const double q2 = q * q;
   auto fn = [&](double r) { return r * r - 3.0 * r + 2.0 * q2 + sign * 2.0 * std::fabs(a) * std::sqrt(r - q2); };
-  double hi = 4.0 + 2.0 * std::fabs(a), lo = std::fmax(q2, 0.0) + 1e-12;
-  // fn(hi) > 0 for the outer root; walk lo up until it is below the root
+  double hi = 6.0;
   double probe = hi;
-  for (int i = 0; i < 400 && fn(probe) > 0.0; ++i) probe -= 0.01;
-  if (fn(probe) > 0.0) return std::numeric_limits<double>::quiet_NaN();
-  lo = probe;
+  while (probe > q2 + 1e-9 && fn(probe) > 0.0) {
+    hi = probe;
+    probe -= 0.005;
+  }
+  if (!(probe > q2) || fn(probe) > 0.0) return std::numeric_limits<double>::quiet_NaN();
+  double lo = probe;
   for (int i = 0; i < 200; ++i) {
     const double mid = 0.5 * (lo + hi);
     if (fn(mid) > 0.0) hi = mid;
@@ -281,8 +285,10 @@ glc_status pack_scene(const glc_scene_input& in, glc_scene& out) {
   out.surface_inner = in.has_surface ? in.surface_inner / M : 0.0;
   out.surface_outer = in.has_surface ? in.surface_outer / M : 0.0;
   out.intensity_at_six = in.has_surface ? in.intensity_at_six : 0.0;
-  out.photon_shell_radius = photon_orbit(a, q, -1.0);
-  if (!std::isfinite(out.photon_shell_radius)) out.photon_shell_radius = 3.0 + 2.0 * std::fabs(a);
+  // inner (prograde) circular photon orbit: the MIXED binary64 shell r < factor * r_ph hugs the
+  // horizon and the co-rotating photon sphere
+  out.photon_shell_radius = photon_orbit(a, q, +1.0);
+  if (!std::isfinite(out.photon_shell_radius)) out.photon_shell_radius = 3.0 - 2.0 * std::fabs(a);
   out.isco_prograde = out.extremality == 2 ? std::numeric_limits<double>::quiet_NaN() : prograde_isco(a, q);
   double ev[4], tg[4];
   for (int i = 0; i < 4; ++i) {

@@ -17,6 +17,8 @@
 //          in double; the event path and the final null-constraint renormalisation are double.
 #pragma once
 
+#include <type_traits>
+
 #include "glc_dp54.cuh"
 #include "../../include/glc.h"
 
@@ -149,32 +151,59 @@ struct RayResult {
   S surface_r, surface_phi, g;
 };
 
-// Bisection on the dense output (geodesic.rs:640-676). value_at(y, v) -> false on failure.
-template <class T, class F>
-GLC_HD bool localize(const T y0[6], T h, const T K[7][7], T tol, T sv, T ev, F value_at, T& theta, T yroot[6],
+// Root of an event function on the dense output between theta = 0 (value sv) and 1 (value ev).
+// The reference's oracle bisects to the affine tolerance (geodesic.rs:640-676); this is the
+// Illinois variant of regula falsi with a bisection guard, which reaches the same bracket width in
+// a handful of evaluations. Like the oracle, it stops once the bracket, in affine units, is within
+// `tol` and returns the bracket end with the smaller |value|. value_at(y, v) -> false on failure.
+template <class T, class TK, class F>
+GLC_HD bool localize(const T y0[6], T h, const TK K[7][7], T tol, T sv, T ev, F value_at, T& theta, T yroot[6],
                      T& bracket) {
-  T lower = T(0), upper = T(1), lv = sv, uv = ev;
+  T lo = T(0), hi = T(1), flo = sv, fhi = ev;  // true values at the bracket ends
+  T slo = sv, shi = ev;                        // Illinois-scaled values used for interpolation
+  int side = 0;
+  T width2 = T(2);  // bracket width two iterations ago
+  T width1 = T(1);
   const T ah = g_abs(h);
   for (int i = 0; i < 64; ++i) {
-    if ((upper - lower) * ah <= tol) break;
-    const T mid = T(0.5) * (lower + upper);
-    if (mid == lower || mid == upper) break;
+    const T width = hi - lo;
+    if (width * ah <= tol) break;
+    T mid;
+    if (width > T(0.5) * width2) {
+      mid = T(0.5) * (lo + hi);  // guard: the bracket stopped halving
+      width2 = T(2) * width;
+    } else {
+      mid = (lo * shi - hi * slo) / (shi - slo);
+      if (!(mid > lo && mid < hi)) mid = T(0.5) * (lo + hi);
+      width2 = width1;
+    }
+    width1 = width;
+    if (mid == lo || mid == hi) break;
     T ys[6], dt;
-    dense_eval(y0, h, K, mid, ys, dt);
+    dense_eval_mixed(y0, h, K, mid, ys, dt);
     T v;
     if (!value_at(ys, v)) return false;
-    if (g_signbit(lv) == g_signbit(v)) {
-      lower = mid;
-      lv = v;
+    if (g_signbit(flo) == g_signbit(v)) {
+      lo = mid;
+      flo = slo = v;
+      if (side == -1) shi *= T(0.5);
+      side = -1;
     } else {
-      upper = mid;
-      uv = v;
+      hi = mid;
+      fhi = shi = v;
+      if (side == 1) slo *= T(0.5);
+      side = 1;
+    }
+    if (v == T(0)) {
+      lo = hi = mid;
+      flo = fhi = v;
+      break;
     }
   }
-  theta = g_abs(lv) <= g_abs(uv) ? lower : upper;
+  theta = g_abs(flo) <= g_abs(fhi) ? lo : hi;
   T dt;
-  dense_eval(y0, h, K, theta, yroot, dt);
-  bracket = (upper - lower) * ah;
+  dense_eval_mixed(y0, h, K, theta, yroot, dt);
+  bracket = (hi - lo) * ah;
   for (int c = 0; c < 6; ++c)
     if (!g_finite(yroot[c])) return false;
   return true;
@@ -245,12 +274,45 @@ GLC_HD bool renormalize_null(const KN<T>& k, T y[6], T E) {
 template <int P>
 struct Ray;
 
+// One binary64 DP5(4) attempt from a binary64 state (k1 evaluated at y0).
+struct Attempt64 {
+  double inc[6], k7[7];
+  double dt, r_end, vr_end, en;
+  Invariants<double> inv;
+  bool finite;
+};
+
+GLC_HD void attempt64_body(const KN<double>& kd, const double y0[6], double E, double h, double t_start,
+                           const Tolerance& tol, Attempt64* a) {
+  double k1[7], rr, vv;
+  kn_rhs(kd, y0, E, k1, rr, vv);
+  a->en = dp5_attempt<double, double>(kd, y0, E, h, k1, t_start, tol, a->inc, a->dt, a->k7, a->r_end, a->vr_end,
+                                      a->inv, a->finite);
+}
+
 #if defined(__CUDA_ARCH__)
-template <int P>
+__device__ __noinline__ void attempt64_outline(KN<double> kd, const double* y0, double E, double h, double t_start,
+                                               Tolerance tol, Attempt64* a) {
+  attempt64_body(kd, y0, E, h, t_start, tol, a);
+}
+GLC_HD void attempt64(const KN<double>& kd, const double y0[6], double E, double h, double t_start,
+                      const Tolerance& tol, Attempt64* a) {
+  attempt64_outline(kd, y0, E, h, t_start, tol, a);
+}
+#else
+GLC_HD void attempt64(const KN<double>& kd, const double y0[6], double E, double h, double t_start,
+                      const Tolerance& tol, Attempt64* a) {
+  attempt64_body(kd, y0, E, h, t_start, tol, a);
+}
+#endif
+
+#if defined(__CUDA_ARCH__)
+template <int P, int K64>
 __device__ __noinline__ bool rare_step_outline(Ray<P>& ray, const LaneScene& sc, const glc_policy& pol,
                                                RayResult<typename PrecTraits<P>::S>& res,
                                                typename PrecTraits<P>::C en) {
-  return ray.rare_step(sc, pol, res, en, false);
+  using TK = typename std::conditional<K64 != 0, double, typename PrecTraits<P>::C>::type;
+  return ray.template rare_step<TK>(sc, pol, res, en);
 }
 #endif
 
@@ -372,34 +434,24 @@ struct Ray {
     bool finite;
     const bool stepped64 = P == kMIXED && kUse64;
     if (stepped64) {
-      // binary64 step inside the shell: double k1 at y, double stages and error control
-      const KN<double> kd = sc.kn;
-      double yd[6], k1d[7], rr, vv, incd[6], dtd, k7d[7], red, vred;
-      Invariants<double> invd;
+      // binary64 step inside the shell: double k1 at y, double stages and error control (out of
+      // line on the device, so the binary32 hot loop is not register-allocated for it)
+      Attempt64 a;
+      double yd[6];
       for (int c = 0; c < 6; ++c) yd[c] = double(y[c]);
-      kn_rhs(kd, yd, double(E), k1d, rr, vv);
-      const double end = dp5_attempt<double, double>(kd, yd, double(E), double(h), k1d, double(tsum + tcorr), tol,
-                                                     incd, dtd, k7d, red, vred, invd, finite);
-      for (int c = 0; c < 6; ++c) inc[c] = S(incd[c]);
-      for (int c = 0; c < 7; ++c) k7[c] = C(k7d[c]);
-      dt = C(dtd);
-      r_end = S(red);
-      vr_end = S(vred);
-      inv.lz = C(invd.lz);
-      inv.carter = C(invd.carter);
-      inv.null_residual = C(invd.null_residual);
-      en = C(end);
-      if (finite && end <= 1.0) {
-        // drifts from the binary64 evaluation
-        update_drifts(invd);
-        inv.null_residual = C(NAN);  // already folded in
-      }
+      attempt64(sc.kn, yd, double(E), double(h), double(tsum + tcorr), tol, &a);
+      for (int c = 0; c < 6; ++c) inc[c] = S(a.inc[c]);
+      for (int c = 0; c < 7; ++c) k7[c] = C(a.k7[c]);
+      dt = C(a.dt);
+      r_end = S(a.r_end);
+      vr_end = S(a.vr_end);
+      en = C(a.en);
+      finite = a.finite;
+      if (finite && a.en <= 1.0) update_drifts(a.inv);  // drifts from the binary64 evaluation
     } else {
       const KN<C> kc = kn_cast<C>(sc.kn);
       C incc[6], rec, vrec;
-      // MIXED evaluates the invariants in binary64 at the committed state instead
-      en = dp5_attempt<C, S, P != kMIXED>(kc, y, C(E), h, k1, C(tsum + tcorr), tol, incc, dt, k7, rec, vrec,
-                                          inv, finite);
+      en = dp5_attempt<C, S, true>(kc, y, C(E), h, k1, C(tsum + tcorr), tol, incc, dt, k7, rec, vrec, inv, finite);
       for (int c = 0; c < 6; ++c) inc[c] = S(incc[c]);
       r_end = S(rec);
       vr_end = S(vrec);
@@ -449,19 +501,28 @@ struct Ray {
       LaneScene lsc = sc;
       glc_policy pl = pol;
       RayResult<S> rs;
-      const bool done = rare_step_outline<P>(tmp, lsc, pl, rs, en);
+      const bool done = rare_step_outline<P, stepped64 ? 1 : 0>(tmp, lsc, pl, rs, en);
       *this = tmp;
       if (done) res = rs;
       return done;
 #else
-      return rare_step(sc, pol, res, en, stepped64);
+      if (stepped64) return rare_step<double>(sc, pol, res, en);
+      return rare_step<C>(sc, pol, res, en);
 #endif
     }
     // ---- plain commit
     CompSum::add(tsum, tcorr, S(dt));
     commit_azimuth(y, yend);
     if constexpr (P == kMIXED) {
-      if (!stepped64) update_drifts(kn_invariants_mixed(sc.kn, yend, double(E), float(r_end)));
+      // L_z and Carter's constant cancel badly in binary32 far out; re-evaluate them in binary64
+      // at the binary64 state (the null residual keeps its binary32 value)
+      if (!stepped64) {
+        const Invariants<double> i64 = kn_invariants_mixed(sc.kn, yend, double(E), float(r_end));
+        inv.lz = i64.lz;
+        inv.carter = i64.carter;
+        Invariants<double> m{i64.lz, i64.carter, double(inv.null_residual)};
+        update_drifts(m);
+      }
     } else {
       update_drifts(inv);
     }
@@ -488,22 +549,37 @@ struct Ray {
   // localize events, turning points and equatorial crossings and commit. The sign tests use the
   // stored start values (r, vr: what the previous step's end checks used), so a crossing is never
   // lost between a binary32 detection and a binary64 re-check.
-  GLC_HD bool rare_step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, C en, bool stepped64) {
+  // TK is the stage precision of the event path: the stepping precision (binary32 in MIXED
+  // outside the shell, binary64 on shell steps); the dense state, the event functions and the
+  // committed state are in S.
+  template <class TK>
+  GLC_HD bool rare_step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, C en) {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
-    T K[7][7];
+    const KN<TK> kk = kn_cast<TK>(sc.kn);
+    TK K[7][7];
+    TK yk[6];
+    for (int c = 0; c < 6; ++c) yk[c] = TK(y[c]);
     {
-      T rr, vv;
-      if (P == kMIXED) {
-        kn_rhs(kt, y, E, K[0], rr, vv);
+      TK rr, vv;
+      if (P == kMIXED && sizeof(TK) == sizeof(double)) {
+        kn_rhs(kk, yk, TK(E), K[0], rr, vv);  // shell step: binary64 k1
       } else {
-        for (int c = 0; c < 7; ++c) K[0][c] = T(k1[c]);
+        for (int c = 0; c < 7; ++c) K[0][c] = TK(k1[c]);
       }
     }
     const T r0 = T(r), vr0 = T(vr);
     const T hh = T(h);
-    T yend[6], r_end, vr_end;
-    dp5_stages(kt, y, E, hh, K, yend, r_end, vr_end);
+    TK yend_k[6], rk, vrk;
+    dp5_stages(kk, yk, TK(E), TK(h), K, yend_k, rk, vrk);
+    T yend[6], r_end;
+    {
+      T dtd;
+      dense_eval_mixed(y, hh, K, T(1), yend, dtd);
+      int gs;
+      r_end = sizeof(TK) == sizeof(T) ? T(rk) : kn_radius(kt, yend[0], yend[1], yend[2], gs);
+    }
+    const T vr_end = T(vrk);
     const double guard = pol.singularity_guard;
     const T tol = T(pol.event_affine_tolerance);
     bool fail = false;
@@ -565,9 +641,10 @@ struct Ray {
       if ((sv < T(0) && evv >= T(0)) || (sv > T(0) && evv <= T(0))) {
         T th, yr[6], br;
         auto vr_at = [&](const T* ys, T& v) -> bool {
-          T d[7], rr, vv;
-          kn_rhs(kt, ys, E, d, rr, vv);
-          v = T(dir) * vv;
+          TK d[7], rr, vv, yy[6];
+          for (int c = 0; c < 6; ++c) yy[c] = TK(ys[c]);
+          kn_rhs(kk, yy, TK(E), d, rr, vv);
+          v = T(dir) * T(vv);
           return g_finite(v);
         };
         if (localize(y, hh, K, tol, sv, evv, vr_at, th, yr, br) && (!has_event || th < term_theta)) {
@@ -593,7 +670,7 @@ struct Ray {
     T ycommit[6], dtc;
     {
       T ytmp[6];
-      dense_eval(y, hh, K, term_theta, ytmp, dtc);
+      dense_eval_mixed(y, hh, K, term_theta, ytmp, dtc);
       for (int c = 0; c < 6; ++c) ycommit[c] = has_event ? states[first][c] : yend[c];
     }
     CompSum::add(tsum, tcorr, dtc);
@@ -621,7 +698,6 @@ struct Ray {
     vr = vr_end;
     arm_update(sc, pol);
     h = dir * next_step(pol, g_abs(h), en, true);
-    (void)stepped64;
     return false;
   }
 

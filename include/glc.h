@@ -109,7 +109,7 @@ typedef struct glc_scene {
   double horizon_event_radius;    /* r_+ + offset */
   double escape_radius;           /* 0 when not installed */
   double surface_inner, surface_outer, intensity_at_six;
-  double photon_shell_radius;     /* outer (retrograde) equatorial photon orbit radius */
+  double photon_shell_radius;     /* inner (prograde) equatorial photon orbit radius */
   double isco_prograde;           /* prograde ISCO radius (informational) */
   double observer_txyz[4];
   double four_velocity[4], image_right[4], image_up[4], arrival[4];
@@ -131,7 +131,7 @@ typedef struct glc_policy {
   uint32_t maximum_consecutive_rejects;
   int32_t precision;              /* glc_precision */
   double event_affine_tolerance, event_tie_tolerance, event_arming_band, singularity_guard;
-  double mixed_shell_factor;      /* MIXED: binary64 steps while r < factor * photon shell radius */
+  double mixed_shell_factor;      /* MIXED: binary64 steps while r < factor * prograde photon orbit */
   uint32_t renormalize_null;      /* MIXED: renormalize the final momentum onto H = 0 */
   uint32_t persistent;            /* 1: persistent work-queue kernel, 0: one thread per ray */
   uint32_t block_threads;         /* threads per block (multiple of 32) */

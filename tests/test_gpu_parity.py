@@ -194,3 +194,18 @@ def test_full_hd_frame_never_exhausts_steps(pipe, precision):
     assert hist[G.Termination.NUMERICAL_FAILURE] == 0, hist
     assert hist[0] == 0  # every pixel written
     assert d["accepted_steps"].max() < 20000
+
+
+def test_mixed_is_at_or_below_plain_fp32_error_on_every_observable(pipe, config1_oracle):
+    """The precision study's acceptance: at the same frame policy, MIXED errors against the binary64
+    oracle are no larger than plain binary32's (the null residual, which both runs carry at the
+    tolerance level, within 25 %)."""
+    obs, sel, ref = config1_oracle
+    m = compare(run_image(pipe, obs, G.Precision.MIXED), sel, ref)
+    f = compare(run_image(pipe, obs, G.Precision.FP32), sel, ref)
+    print("mixed", m, "fp32", f)
+    assert m["class_mismatch"] <= f["class_mismatch"]
+    for k in ("escape_direction_rad", "g_rel", "hit_radius", "source_azimuth", "travel_time", "max_lz_drift",
+              "max_carter_drift"):
+        assert m[k] <= f[k], (k, m[k], f[k])
+    assert m["max_null_residual"] <= 1.25 * f["max_null_residual"]
