@@ -160,9 +160,11 @@ GLC_HD T kn_radius(const KN<T>& k, T x, T y, T z, int& status) {
 // Reduced right-hand side. y = (x, y, z, p_x, p_y, p_z); d = (x', y', z', p_x', p_y', p_z', t').
 // Also returns r and the radial velocity dr/dlambda = grad(r) . x'. Non-finite values propagate
 // as NaN into the step's error norm, which the stepper turns into a numerical failure.
+// L_z, Carter's constant, the normalized null residual and the spin term of Carter's constant
+// (Q = L_x^2 + L_y^2 + abracket, see kn_invariants).
 template <class T>
 struct Invariants {
-  T lz, carter, null_residual;
+  T lz, carter, null_residual, abracket;
 };
 
 // kInv: also evaluate L_z, Carter's constant and the normalized null residual at this point from
@@ -223,12 +225,14 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
   r_out = r;
   vr_out = grx * vx + gry * vy + grz * vz;
   if (kInv) {
-    // Carter's constant in the axis-regular Cartesian form (see kn_invariants)
+    // Carter's constant as Q = L_x^2 + L_y^2 + a^2 [(z^2/r^2)(P_perp^2 - E^2) - (rho^2/A) p_z^2]
+    // (see kn_invariants): no r^2-sized terms cancel, so binary32 keeps its relative accuracy far out
     const T rho2 = x * x + yy * yy;
-    const T Sxy = x * px + yy * py;
     const T pp2 = px * px + py * py;
+    const T Lx = yy * pz - z * py, Ly = z * px - x * pz;
     inv->lz = x * py - yy * px;
-    inv->carter = z * z * inv_r2 * (A * pp2 - k.a2 * E * E) - T(2) * z * Sxy * pz + r2 * rho2 * inv_A * pz * pz;
+    inv->abracket = k.a2 * (z * z * inv_r2 * (pp2 - E * E) - rho2 * inv_A * pz * pz);
+    inv->carter = Lx * Lx + Ly * Ly + inv->abracket;
     // g^{mu nu} p_mu p_nu with m = eta - f l l and u_i = l^i p_i (u_0 = E): diagonal terms
     // eta_ii p_i^2 - f u_i^2, off-diagonal -f u_i u_j
     const T u1 = lx * px, u2 = ly * py, u3 = lz * pz;
@@ -242,11 +246,13 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
 }
 
 // Conserved quantities and the normalized null residual (the reference's drift diagnostics,
-// crates/gravlume-domain/src/spacetime.rs:345-401 and numerics.rs:3-35). Carter's constant uses
-// the axis-regular Cartesian form
-//   Q = (z^2 / r^2) (A P_perp^2 - a^2 E^2) - 2 z S p_z + (r^2 rho^2 / A) p_z^2,
-//   S = x p_x + y p_y, P_perp^2 = p_x^2 + p_y^2, rho^2 = x^2 + y^2,
-// which equals the oracle's trigonometric form p_theta^2 + cos^2(theta)(L_z^2/sin^2 - a^2 E^2).
+// crates/gravlume-domain/src/spacetime.rs:345-401 and numerics.rs:3-35). Carter's constant uses the
+// Cartesian form
+//   Q = L_x^2 + L_y^2 + a^2 [(z^2 / r^2)(P_perp^2 - E^2) - (rho^2 / A) p_z^2],
+//   L = x cross p, P_perp^2 = p_x^2 + p_y^2, rho^2 = x^2 + y^2, A = r^2 + a^2,
+// which equals the oracle's trigonometric form p_theta^2 + cos^2(theta)(L_z^2/sin^2 - a^2 E^2)
+// identically (z^2 P_perp^2 - 2 z (x p_x + y p_y) p_z + rho^2 p_z^2 = L_x^2 + L_y^2) and is regular
+// on the axis.
 template <class T>
 GLC_HD Invariants<T> kn_invariants(const KN<T>& k, const T y[6], T E, T r) {
   const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
@@ -255,9 +261,10 @@ GLC_HD Invariants<T> kn_invariants(const KN<T>& k, const T y[6], T E, T r) {
   const T r2 = r * r;
   const T A = r2 + k.a2;
   const T rho2 = x * x + yy * yy;
-  const T S = x * px + yy * py;
   const T pp2 = px * px + py * py;
-  out.carter = (z * z / r2) * (A * pp2 - k.a2 * E * E) - T(2) * z * S * pz + (r2 * rho2 / A) * pz * pz;
+  const T Lx = yy * pz - z * py, Ly = z * px - x * pz;
+  out.abracket = k.a2 * (z * z / r2 * (pp2 - E * E) - rho2 / A * pz * pz);
+  out.carter = Lx * Lx + Ly * Ly + out.abracket;
   // g^{mu nu} p_mu p_nu with g^{mu nu} = eta - f l l, p = (-E, p_x, p_y, p_z), l = (-1, l_x, l_y, l_z).
   const T inv_r = T(1) / r;
   const T sigma = r2 + k.a2 * z * z / r2;
@@ -288,26 +295,35 @@ GLC_HD double rcp_refined(double x) {
   return r0 * (2.0 - x * r0);
 }
 
-// Binary64 L_z and Carter's constant at a binary64 state, with r^2 seeded by the binary32
-// right-hand side at the same point (r_hint) and refined by one Newton step on
-// u^2 - b u - a^2 z^2 = 0 (u = r^2); null_residual is left at 0 for the caller to fill.
-GLC_HD Invariants<double> kn_invariants_mixed(const KN<double>& k, const double y[6], double E, float r_hint) {
-  const double x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
-  const double b = x * x + yy * yy + z * z - k.a2;
-  const double az2 = k.a2 * z * z;
-  double u = double(r_hint) * double(r_hint);
-  u -= (u * u - b * u - az2) * double(g_rcp(float(2.0 * u - b)));
-  const double inv_r2 = rcp_refined(u);
-  const double A = u + k.a2;
-  const double inv_A = rcp_refined(A);
-  const double rho2 = x * x + yy * yy;
-  const double Sxy = x * px + yy * py;
-  const double pp2 = px * px + py * py;
-  Invariants<double> inv;
-  inv.lz = x * py - yy * px;
-  inv.carter = z * z * inv_r2 * (A * pp2 - k.a2 * E * E) - 2.0 * z * Sxy * pz + u * rho2 * inv_A * pz * pz;
-  inv.null_residual = 0.0;
-  return inv;
+// ---- compensated binary32 (a pair hi + lo with |lo| <= ulp(hi) / 2) ----
+// TwoSum (Knuth): s + e == a + b exactly.
+GLC_HD void two_sum(float a, float b, float& s, float& e) {
+  s = a + b;
+  const float bv = s - a;
+  e = (a - (s - bv)) + (b - bv);
+}
+// hi + lo += v, renormalized.
+GLC_HD void ff_add(float& hi, float& lo, float v) {
+  float s, e;
+  two_sum(hi, v, s, e);
+  e += lo;
+  hi = s + e;
+  lo = e - (hi - s);
+}
+// (ah + al)(bh + bl) as a pair; the al * bl term is below the pair's precision.
+GLC_HD void ff_mul(float ah, float al, float bh, float bl, float& ph, float& pl) {
+  const float p = ah * bh;
+  const float e = fmaf(ah, bh, -p);
+  pl = e + (ah * bl + al * bh);
+  ph = p + pl;
+  pl = pl - (ph - p);
+}
+// Cross-product component a1 b2 - a2 b1 of pairs, returned as a float accurate to its own scale.
+GLC_HD float ff_cross(float a1h, float a1l, float b2h, float b2l, float a2h, float a2l, float b1h, float b1l) {
+  float p1h, p1l, p2h, p2l;
+  ff_mul(a1h, a1l, b2h, b2l, p1h, p1l);
+  ff_mul(a2h, a2l, b1h, b1l, p2h, p2l);
+  return (p1h - p2h) + (p1l - p2l);
 }
 
 }  // namespace glc

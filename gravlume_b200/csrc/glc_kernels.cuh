@@ -105,20 +105,37 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
         make_int4(int(ray.turnings), int(ray.crossings), ray.winding, ray.turn_r == ray.turn_r ? 1 : 0);
   if (o.escape) reinterpret_cast<double2*>(o.escape)[slot] = make_double2(double(res.escape_theta), double(res.escape_phi));
   if (o.surface) reinterpret_cast<double2*>(o.surface)[slot] = make_double2(double(res.surface_r), double(res.surface_phi));
-  const S travel = ray.dir * (ray.tsum + ray.tcorr);
+  const S travel = ray.travel();
   if (o.redshift_time) reinterpret_cast<double2*>(o.redshift_time)[slot] = make_double2(double(res.g), double(travel));
-  if (o.event) reinterpret_cast<double2*>(o.event)[slot] = make_double2(double(res.event_residual), double(ray.affine));
+  if (o.event) reinterpret_cast<double2*>(o.event)[slot] = make_double2(double(res.event_residual), double(ray.affine()));
   if (o.drift_a) reinterpret_cast<double2*>(o.drift_a)[slot] = make_double2(double(ray.dnull), 0.0);
   if (o.drift_b) reinterpret_cast<double2*>(o.drift_b)[slot] = make_double2(double(ray.dlz), double(ray.dq));
   if (o.turning)
     reinterpret_cast<double2*>(o.turning)[slot] = make_double2(double(ray.turn_r), double(ray.azimuth_advance()));
-  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = make_double2(double(ray.y[0]), double(ray.y[1]));
+  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = make_double2(double(ray.ys(0)), double(ray.ys(1)));
   if (o.position_zr) {
     int gs;
-    const double r = kn_radius(ls.kn, double(ray.y[0]), double(ray.y[1]), double(ray.y[2]), gs);
-    reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(ray.y[2]), r);
+    const double r = kn_radius(ls.kn, double(ray.ys(0)), double(ray.ys(1)), double(ray.ys(2)), gs);
+    reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(ray.ys(2)), r);
   }
 }
+
+// Register budget per precision: binary32 fits 128 registers (16 warps per SM); the binary64 and
+// mixed kernels carry binary64 event and shell paths and run at 2 blocks of 128 threads per SM.
+#ifndef GLC_MIN_BLOCKS_FP32
+#define GLC_MIN_BLOCKS_FP32 4
+#endif
+#ifndef GLC_MIN_BLOCKS_MIXED
+#define GLC_MIN_BLOCKS_MIXED 2
+#endif
+#ifndef GLC_MIN_BLOCKS_FP64
+#define GLC_MIN_BLOCKS_FP64 2
+#endif
+template <int P>
+struct LaunchShape {
+  static constexpr int kMinBlocks =
+      P == kFP32 ? GLC_MIN_BLOCKS_FP32 : (P == kMIXED ? GLC_MIN_BLOCKS_MIXED : GLC_MIN_BLOCKS_FP64);
+};
 
 template <int P>
 __device__ __forceinline__ bool ray_step(Ray<P>& ray, const LaneScene& ls, const glc_policy& pol,
@@ -129,7 +146,7 @@ __device__ __forceinline__ bool ray_step(Ray<P>& ray, const LaneScene& ls, const
 
 // One thread per ray; rays in tile order so a warp covers a compact pixel tile.
 template <int P>
-__global__ void __launch_bounds__(128) trace_simple_kernel(JobView job, glc_policy pol, glc_results out) {
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out) {
   using S = typename PrecTraits<P>::S;
   const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= job.total) return;
@@ -151,10 +168,12 @@ __global__ void __launch_bounds__(128) trace_simple_kernel(JobView job, glc_poli
 
 // Persistent kernel: every warp loops until the job's queue is drained. Idle lanes are refilled
 // from a warp-private range of `rays_per_grab` consecutive ray indices taken from a global atomic
-// counter, every `refill_interval` steps (or at once when the whole warp is idle). The counter is
-// the only scratch memory; the loop has no waits on other warps or blocks.
+// counter. A refill happens on every `refill_interval`-th step once at least `refill_min_idle`
+// lanes are idle (or at once when the whole warp is idle), so ray set-up runs for several lanes
+// together rather than diverging lane by lane. The counter is the only scratch memory; the loop
+// has no waits on other warps or blocks.
 template <int P>
-__global__ void __launch_bounds__(128) trace_persistent_kernel(JobView job, glc_policy pol, glc_results out,
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persistent_kernel(JobView job, glc_policy pol, glc_results out,
                                                                unsigned long long* queue) {
   using S = typename PrecTraits<P>::S;
   const unsigned FULL = 0xffffffffu;
@@ -169,11 +188,12 @@ __global__ void __launch_bounds__(128) trace_persistent_kernel(JobView job, glc_
   bool drained = false;
   const unsigned grab = pol.rays_per_grab < 32 ? 32u : pol.rays_per_grab;
   const unsigned interval = pol.refill_interval == 0 ? 1u : pol.refill_interval;
+  const unsigned min_idle = pol.refill_min_idle == 0 ? 1u : (pol.refill_min_idle > 32 ? 32u : pol.refill_min_idle);
   unsigned iter = 0;
   for (;;) {
-    const bool any_active = __any_sync(FULL, active);
-    if (!drained && (!any_active || iter % interval == 0u)) {
-      unsigned idle = __ballot_sync(FULL, !active);
+    unsigned idle = __ballot_sync(FULL, !active);
+    const bool any_active = idle != FULL;
+    if (!drained && (!any_active || (iter % interval == 0u && unsigned(__popc(idle)) >= min_idle))) {
       while (idle != 0u) {
         if (grab_next >= grab_end) {
           unsigned long long base = 0;

@@ -317,22 +317,26 @@ __device__ __noinline__ bool rare_step_outline(Ray<P>& ray, const LaneScene& sc,
 #endif
 
 // ----------------------------------------------------------------------------------------------
-// One ray's trace state. S holds the state accumulators; bookkeeping that needs no more than the
-// stepping precision (step size, event values, drifts) is kept in C.
+// One ray's trace state. The state (x, y, z, p_x, p_y, p_z), affine parameter and coordinate time
+// are stepping-precision values; MIXED keeps each as a compensated binary32 pair (hi + lo, ~48
+// significant bits) so that its accumulation error matches binary64 without binary64 arithmetic in
+// the hot loop. S is the precision of the event path and observables (binary64 in MIXED).
 template <int P>
 struct Ray {
   using S = typename PrecTraits<P>::S;
   using C = typename PrecTraits<P>::C;
+  static constexpr bool kPair = P == kMIXED;
 
-  S y[6];
-  S E;
-  S affine;
-  S tsum, tcorr;
-  S az0;          // initial azimuth; the advance is az_end - az0 + 2 pi * winding
+  C yh[6], yl[6];  // state (yl: MIXED low parts, zero otherwise)
+  C ah, al;        // affine parameter
+  C th, tl;        // coordinate-time increment sum (compensated in every mode, like the reference)
+  C Ec;            // energy in stepping precision
+  S E;             // energy for the event path and observables
+  S az0;           // initial azimuth; the advance is az_end - az0 + 2 pi * winding
   C h;
-  C k1[7];        // FSAL derivative at y (precision C; MIXED recomputes it in double on shell steps)
-  S r, vr;        // event-function inputs at y: the exact values the previous step's checks used
-                  // (storage precision, so a binary64 re-check's sign survives being stored)
+  C k1[7];         // FSAL derivative at the state
+  S r, vr;         // event-function inputs at the state: the exact values the previous step's checks
+                   // used (kept in S, so a binary64 re-check's sign survives being stored)
   C lz0, q0, dnull, dlz, dq;
   C turn_r;
   C dir;
@@ -343,34 +347,48 @@ struct Ray {
   uint32_t flags;
   bool have_inv;
 
-  GLC_HD void init(const LaneScene& sc, const glc_policy& pol, const double st8[8], double direction) {
-    for (int c = 0; c < 3; ++c) {
-      y[c] = S(st8[1 + c]);
-      y[3 + c] = S(st8[5 + c]);
+  GLC_HD S ys(int c) const { return kPair ? S(yh[c]) + S(yl[c]) : S(yh[c]); }
+  GLC_HD void state_s(S out[6]) const {
+    for (int c = 0; c < 6; ++c) out[c] = ys(c);
+  }
+  GLC_HD void set_state(const S v[6]) {
+    for (int c = 0; c < 6; ++c) {
+      yh[c] = C(v[c]);
+      yl[c] = kPair ? C(v[c] - S(yh[c])) : C(0);
     }
+  }
+  GLC_HD S travel() const { return S(dir) * (S(th) + S(tl)); }
+  GLC_HD S affine() const { return kPair ? S(ah) + S(al) : S(ah); }
+
+  GLC_HD void init(const LaneScene& sc, const glc_policy& pol, const double st8[8], double direction) {
+    S v[6];
+    for (int c = 0; c < 3; ++c) {
+      v[c] = S(st8[1 + c]);
+      v[3 + c] = S(st8[5 + c]);
+    }
+    set_state(v);
     E = S(-st8[4]);
+    Ec = C(E);
     dir = C(direction);
     h = dir * C(pol.initial_step);
-    affine = S(0);
-    tsum = S(0);
-    tcorr = S(0);
+    ah = al = th = tl = C(0);
     accepted = rejected = f64steps = consecutive = 0;
     turnings = crossings = 0;
     winding = 0;
     flags = 0;
     polar = st8[3] > 0.0 ? 1 : (st8[3] < 0.0 ? -1 : 0);
     turn_r = C(NAN);
-    az0 = g_atan2(y[1], y[0]);
+    az0 = g_atan2(v[1], v[0]);
     dnull = dlz = dq = C(0);
     // first derivative (FSAL seed), the invariants at the start and the event arming
     // (geodesic.rs:98-136, 536-544)
     const KN<C> kc = kn_cast<C>(sc.kn);
-    C yc[6], rr, vv;
+    C rr, vv;
     Invariants<C> inv;
-    for (int c = 0; c < 6; ++c) yc[c] = C(y[c]);
-    kn_rhs<C, true>(kc, yc, C(E), k1, rr, vv, &inv);
+    kn_rhs<C, true>(kc, yh, Ec, k1, rr, vv, &inv);
     r = S(rr);
     vr = S(vv);
+    if (kPair) pair_invariants(inv);
     have_inv = g_finite(rr) && g_finite(inv.lz) && g_finite(inv.carter) && g_finite(inv.null_residual);
     lz0 = inv.lz;
     q0 = inv.carter;
@@ -378,9 +396,20 @@ struct Ray {
     if (have_inv) {
       dnull = inv.null_residual;
       for (int kind = 0; kind < 4; ++kind) {
-        const S v = event_value<S>(kind, sc, pol.singularity_guard, r, y[2]);
-        if (event_clears_band(kind, v, S(pol.event_arming_band))) armed |= 1u << kind;
+        const S vk = event_value<S>(kind, sc, pol.singularity_guard, r, v[2]);
+        if (event_clears_band(kind, vk, S(pol.event_arming_band))) armed |= 1u << kind;
       }
+    }
+  }
+
+  // MIXED: L_x, L_y, L_z from the compensated state (products of pairs), so that L_z and Carter's
+  // constant keep binary32 relative accuracy in their own scale far from the hole.
+  GLC_HD void pair_invariants(Invariants<C>& inv) const {
+    if constexpr (kPair) {
+      const float lx = ff_cross(yh[1], yl[1], yh[5], yl[5], yh[2], yl[2], yh[4], yl[4]);  // y p_z - z p_y
+      const float ly = ff_cross(yh[2], yl[2], yh[3], yl[3], yh[0], yl[0], yh[5], yl[5]);  // z p_x - x p_z
+      inv.lz = ff_cross(yh[0], yl[0], yh[4], yl[4], yh[1], yl[1], yh[3], yl[3]);          // x p_y - y p_x
+      inv.carter = lx * lx + ly * ly + inv.abracket;
     }
   }
 
@@ -408,16 +437,25 @@ struct Ray {
 
   // Winding of the azimuth about the z axis (geodesic.rs:406-418): a wrap of atan2(y, x) happens
   // only when y changes sign, so the azimuths are evaluated on those steps alone.
-  GLC_HD void commit_azimuth(const S y_old[6], const S y_new[6]) {
-    if (g_signbit(y_old[1]) == g_signbit(y_new[1])) return;
-    const S raw = g_atan2(y_new[1], y_new[0]) - g_atan2(y_old[1], y_old[0]);
+  GLC_HD void commit_azimuth(S x_old, S y_old, S x_new, S y_new) {
+    if (g_signbit(y_old) == g_signbit(y_new)) return;
+    const S raw = g_atan2(y_new, x_new) - g_atan2(y_old, x_old);
     const S pi = S(3.14159265358979323846);
     if (raw > pi) winding -= 1;
     else if (raw < -pi) winding += 1;
   }
 
   GLC_HD S azimuth_advance() const {
-    return g_atan2(y[1], y[0]) - az0 + S(6.28318530717958647692) * S(winding);
+    return g_atan2(ys(1), ys(0)) - az0 + S(6.28318530717958647692) * S(winding);
+  }
+
+  GLC_HD void add_time(C v) { ff_add_any(th, tl, v); }
+  GLC_HD static void ff_add_any(C& hi, C& lo, C v) {
+    if constexpr (sizeof(C) == sizeof(float)) {
+      ff_add(hi, lo, v);
+    } else {
+      CompSum::add(hi, lo, v);
+    }
   }
 
   // Advance by one attempted step. Returns true when the ray terminated (result filled).
@@ -428,31 +466,39 @@ struct Ray {
       return true;
     }
     const Tolerance tol{pol.position_rtol, pol.position_atol, pol.momentum_rtol, pol.momentum_atol};
-    S inc[6], r_end, vr_end;
-    C dt, k7[7], en;
+    C inc[6], dt, k7[7], en;
+    S r_end, vr_end;
     Invariants<C> inv;
     bool finite;
     const bool stepped64 = P == kMIXED && kUse64;
     if (stepped64) {
-      // binary64 step inside the shell: double k1 at y, double stages and error control (out of
-      // line on the device, so the binary32 hot loop is not register-allocated for it)
+      // binary64 step inside the shell: double k1 at the state, double stages and error control
+      // (out of line on the device, so the binary32 hot loop is not register-allocated for it)
       Attempt64 a;
       double yd[6];
-      for (int c = 0; c < 6; ++c) yd[c] = double(y[c]);
-      attempt64(sc.kn, yd, double(E), double(h), double(tsum + tcorr), tol, &a);
-      for (int c = 0; c < 6; ++c) inc[c] = S(a.inc[c]);
+      for (int c = 0; c < 6; ++c) yd[c] = double(ys(c));
+      attempt64(sc.kn, yd, double(E), double(h), double(th) + double(tl), tol, &a);
+      for (int c = 0; c < 6; ++c) inc[c] = C(a.inc[c]);
       for (int c = 0; c < 7; ++c) k7[c] = C(a.k7[c]);
       dt = C(a.dt);
       r_end = S(a.r_end);
       vr_end = S(a.vr_end);
       en = C(a.en);
       finite = a.finite;
-      if (finite && a.en <= 1.0) update_drifts(a.inv);  // drifts from the binary64 evaluation
+      if (finite && a.en <= 1.0) {
+        // exact binary64 increments: commit them through the pair
+        if constexpr (kPair) {
+          for (int c = 0; c < 6; ++c) {
+            const double nv = yd[c] + a.inc[c];
+            inc[c] = C(nv - double(yh[c]) - double(yl[c]));
+          }
+        }
+        update_drifts(a.inv);
+      }
     } else {
       const KN<C> kc = kn_cast<C>(sc.kn);
-      C incc[6], rec, vrec;
-      en = dp5_attempt<C, S, true>(kc, y, C(E), h, k1, C(tsum + tcorr), tol, incc, dt, k7, rec, vrec, inv, finite);
-      for (int c = 0; c < 6; ++c) inc[c] = S(incc[c]);
+      C rec, vrec;
+      en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, inc, dt, k7, rec, vrec, inv, finite);
       r_end = S(rec);
       vr_end = S(vrec);
     }
@@ -480,20 +526,23 @@ struct Ray {
       f64steps += 1;
       flags |= kFlagShellF64;
     }
-    S yend[6];
-    for (int c = 0; c < 6; ++c) yend[c] = y[c] + inc[c];
+    // end-of-step z (the only state component the crossing checks need)
+    C zh = yh[2], zl = yl[2];
+    if constexpr (kPair) ff_add(zh, zl, inc[2]);
+    else zh += inc[2];
+    const S z0 = ys(2), z1 = kPair ? S(zh) + S(zl) : S(zh);
     // ---- crossing detection: start values are exactly the previous step's end values
     const double guard = pol.singularity_guard;
     bool any = false;
     for (int kind = 0; kind < 4; ++kind) {
       if (!((armed >> kind) & 1u) || !((sc.installed >> kind) & 1u)) continue;
-      const S sv = event_value<S>(kind, sc, guard, r, y[2]);
-      const S evv = event_value<S>(kind, sc, guard, r_end, yend[2]);
+      const S sv = event_value<S>(kind, sc, guard, r, z0);
+      const S evv = event_value<S>(kind, sc, guard, r_end, z1);
       any = any || event_crosses(kind, sv, evv);
     }
     const S vs = S(dir) * vr, ve = S(dir) * vr_end;
     any = any || (vs < S(0) && ve >= S(0)) || (vs > S(0) && ve <= S(0));
-    any = any || event_crosses(kEvSurface, y[2], yend[2]);
+    any = any || event_crosses(kEvSurface, z0, z1);
     if (any) {
 #if defined(__CUDA_ARCH__)
       // out-of-line event path on copies, so the hot loop keeps this ray in registers
@@ -511,23 +560,20 @@ struct Ray {
 #endif
     }
     // ---- plain commit
-    CompSum::add(tsum, tcorr, S(dt));
-    commit_azimuth(y, yend);
-    if constexpr (P == kMIXED) {
-      // L_z and Carter's constant cancel badly in binary32 far out; re-evaluate them in binary64
-      // at the binary64 state (the null residual keeps its binary32 value)
-      if (!stepped64) {
-        const Invariants<double> i64 = kn_invariants_mixed(sc.kn, yend, double(E), float(r_end));
-        inv.lz = i64.lz;
-        inv.carter = i64.carter;
-        Invariants<double> m{i64.lz, i64.carter, double(inv.null_residual)};
-        update_drifts(m);
-      }
+    const C x_old = yh[0], y_old = yh[1];
+    add_time(dt);
+    if constexpr (kPair) {
+      for (int c = 0; c < 6; ++c) ff_add(yh[c], yl[c], inc[c]);
+      ff_add(ah, al, h);
     } else {
+      for (int c = 0; c < 6; ++c) yh[c] += inc[c];
+      ah += h;
+    }
+    commit_azimuth(S(x_old), S(y_old), S(yh[0]), S(yh[1]));
+    if (!stepped64) {
+      if (kPair) pair_invariants(inv);
       update_drifts(inv);
     }
-    affine += S(h);
-    for (int c = 0; c < 6; ++c) y[c] = yend[c];
     for (int c = 0; c < 7; ++c) k1[c] = k7[c];
     r = r_end;
     vr = vr_end;
@@ -540,9 +586,20 @@ struct Ray {
     if (armed == 0xFu) return;
     for (int kind = 0; kind < 4; ++kind) {
       if ((armed >> kind) & 1u) continue;
-      const S v = event_value<S>(kind, sc, pol.singularity_guard, r, y[2]);
+      const S v = event_value<S>(kind, sc, pol.singularity_guard, r, ys(2));
       if (event_clears_band(kind, v, S(pol.event_arming_band))) armed |= 1u << kind;
     }
+  }
+
+  GLC_HD void add_time_s(S v) {
+    const C hi = C(v);
+    add_time(hi);
+    if (kPair) add_time(C(v - S(hi)));
+  }
+  GLC_HD void add_affine_s(S v) {
+    const C hi = C(v);
+    ff_add_any(ah, al, hi);
+    if (kPair) ff_add_any(ah, al, C(v - S(hi)));
   }
 
   // Event path in precision S (binary64 in MIXED): recompute the stages for dense output, then
@@ -558,6 +615,8 @@ struct Ray {
     const KN<T> kt = kn_cast<T>(sc.kn);
     const KN<TK> kk = kn_cast<TK>(sc.kn);
     TK K[7][7];
+    T y[6];
+    state_s(y);
     TK yk[6];
     for (int c = 0; c < 6; ++c) yk[c] = TK(y[c]);
     {
@@ -673,16 +732,16 @@ struct Ray {
       dense_eval_mixed(y, hh, K, term_theta, ytmp, dtc);
       for (int c = 0; c < 6; ++c) ycommit[c] = has_event ? states[first][c] : yend[c];
     }
-    CompSum::add(tsum, tcorr, dtc);
-    commit_azimuth(y, ycommit);
+    add_time_s(dtc);
+    commit_azimuth(y[0], y[1], ycommit[0], ycommit[1]);
     {
       int gs;
       const T rr = kn_radius(kt, ycommit[0], ycommit[1], ycommit[2], gs);
       if (gs == kGeomOk) update_drifts(kn_invariants(kt, ycommit, E, rr));
     }
     if (has_event) {
-      affine = hh * term_theta + affine;
-      for (int c = 0; c < 6; ++c) y[c] = ycommit[c];
+      add_affine_s(hh * term_theta);
+      set_state(ycommit);
       const int kind = kinds[first];
       uint32_t term = GLC_TERM_HORIZON;
       if (kind == kEvGuard) term = GLC_TERM_SINGULARITY;
@@ -691,8 +750,8 @@ struct Ray {
       finish_event(sc, pol, res, term, cand, residuals[first]);
       return true;
     }
-    affine += hh;
-    for (int c = 0; c < 6; ++c) y[c] = yend[c];
+    add_affine_s(hh);
+    set_state(yend);
     for (int c = 0; c < 7; ++c) k1[c] = C(K[6][c]);
     r = r_end;
     vr = vr_end;
@@ -717,7 +776,7 @@ struct Ray {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
     T ye[6];
-    for (int c = 0; c < 6; ++c) ye[c] = y[c];
+    state_s(ye);
     if (P == kMIXED && pol.renormalize_null) {
       if (renormalize_null(kt, ye, E)) flags |= kFlagRenormalized;
     }

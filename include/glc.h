@@ -139,6 +139,8 @@ typedef struct glc_policy {
   uint32_t tile_w, tile_h;        /* pixel tile a warp's consecutive rays cover */
   uint32_t refill_interval;       /* persistent: steps between warp refills of finished lanes */
   uint32_t rays_per_grab;         /* persistent: rays a warp takes from the queue per refill (>= 32) */
+  uint32_t refill_min_idle;       /* persistent: idle lanes that trigger a refill (1..32) */
+  uint32_t reserved_policy;
 } glc_policy;
 
 typedef enum glc_camera_kind {

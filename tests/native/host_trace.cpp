@@ -37,15 +37,15 @@ void run(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st
     o[11] = double(res.surface_r);
     o[12] = double(res.surface_phi);
     o[13] = double(res.g);
-    o[14] = double(ray.dir * (ray.tsum + ray.tcorr));
+    o[14] = double(ray.travel());
     o[15] = double(res.event_residual);
-    o[16] = double(ray.affine);
+    o[16] = double(ray.affine());
     o[17] = double(ray.dnull);
     o[18] = double(ray.dlz);
     o[19] = double(ray.dq);
     o[20] = double(ray.turn_r);
     o[21] = double(ray.azimuth_advance());
-    for (int c = 0; c < 6; ++c) o[22 + c] = double(ray.y[c]);
+    for (int c = 0; c < 6; ++c) o[22 + c] = double(ray.ys(c));
     o[28] = ray.f64steps;
   }
 }
