@@ -337,6 +337,7 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
   p.refill_interval = 4;
   p.rays_per_grab = 64;
   p.refill_min_idle = 16;
+  p.mixed_pair_state = 0;
   *out = p;
   return GLC_OK;
 }

@@ -35,6 +35,42 @@ constexpr double d61 = -282668133.0 / 205662961.0, d62 = 2019193451.0 / 61698888
 constexpr double d71 = 40617522.0 / 29380423.0, d72 = -110615467.0 / 29380423.0, d73 = 69997945.0 / 29380423.0;
 }  // namespace dp
 
+// Stage matrix as a table for the compact attempt (row s: coefficients of stages 0..s-1; row 6 is
+// the fifth-order weights, so stage 7's point is the end state), and the error weights b - b*.
+#if defined(__CUDACC__)
+__constant__ double kDpA[7][6] = {
+#else
+static const double kDpA[7][6] = {
+#endif
+    {0, 0, 0, 0, 0, 0},
+    {dp::a21, 0, 0, 0, 0, 0},
+    {dp::a31, dp::a32, 0, 0, 0, 0},
+    {dp::a41, dp::a42, dp::a43, 0, 0, 0},
+    {dp::a51, dp::a52, dp::a53, dp::a54, 0, 0},
+    {dp::a61, dp::a62, dp::a63, dp::a64, dp::a65, 0},
+    {dp::b1, 0, dp::b3, dp::b4, dp::b5, dp::b6},
+};
+#if defined(__CUDACC__)
+__constant__ float kDpAf[7][6] = {
+#else
+static const float kDpAf[7][6] = {
+#endif
+    {0, 0, 0, 0, 0, 0},
+    {float(dp::a21), 0, 0, 0, 0, 0},
+    {float(dp::a31), float(dp::a32), 0, 0, 0, 0},
+    {float(dp::a41), float(dp::a42), float(dp::a43), 0, 0, 0},
+    {float(dp::a51), float(dp::a52), float(dp::a53), float(dp::a54), 0, 0},
+    {float(dp::a61), float(dp::a62), float(dp::a63), float(dp::a64), float(dp::a65), 0},
+    {float(dp::b1), 0, float(dp::b3), float(dp::b4), float(dp::b5), float(dp::b6)},
+};
+
+template <class T>
+GLC_HD T dp_a(int s, int j);
+template <>
+GLC_HD float dp_a<float>(int s, int j) { return kDpAf[s][j]; }
+template <>
+GLC_HD double dp_a<double>(int s, int j) { return kDpA[s][j]; }
+
 struct Tolerance {
   double pos_rtol, pos_atol, mom_rtol, mom_atol;
 };
@@ -94,6 +130,67 @@ GLC_HD C dp5_attempt(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t
     num = larger ? ae : num;
     den = larger ? scale : den;
     chk += err + k7[c];
+  }
+  finite = g_finite(chk);
+  return num * g_rcp(den);
+}
+
+// The same attempt with the stage loop kept rolled: one inlined right-hand side serves all six
+// evaluations and the stages live in a per-thread array (local memory, L1-resident), so the hot
+// loop's instruction footprint is a fraction of the unrolled form's.
+template <class C, class S, bool kInv = true>
+GLC_HD C dp5_attempt_compact(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start,
+                             const Tolerance& tol, C inc[6], C& dt, C k7[7], C& r_end, C& vr_end,
+                             Invariants<C>& inv, bool& finite) {
+  using namespace dp;
+  C K[7][7];
+  C y0c[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) y0c[c] = C(y0[c]);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) K[0][c] = k1[c];
+  C ys[6], rr = C(0), vv = C(0);
+#pragma unroll 1
+  for (int s = 1; s < 7; ++s) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      C w = C(0);
+#pragma unroll 1
+      for (int j = 0; j < s; ++j) w += dp_a<C>(s, j) * K[j][c];
+      ys[c] = y0c[c] + h * w;
+    }
+    C d[7];
+    if (s < 6) {
+      kn_rhs<C, false>(k, ys, E, d, rr, vv);
+    } else {
+      kn_rhs<C, kInv>(k, ys, E, d, rr, vv, &inv);
+    }
+#pragma unroll
+    for (int c = 0; c < 7; ++c) K[s][c] = d[c];
+  }
+  r_end = rr;
+  vr_end = vv;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) inc[c] = ys[c] - y0c[c];
+  dt = h * (C(b1) * K[0][6] + C(b3) * K[2][6] + C(b4) * K[3][6] + C(b5) * K[4][6] + C(b6) * K[5][6]);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) k7[c] = K[6][c];
+  C chk = dt + r_end;
+  if (kInv) chk += inv.lz + inv.carter;
+  C num = C(0), den = C(1);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    const C err =
+        h * (C(e1) * K[0][c] + C(e3) * K[2][c] + C(e4) * K[3][c] + C(e5) * K[4][c] + C(e6) * K[5][c] + C(e7) * K[6][c]);
+    const C sv = c < 6 ? y0c[c] : t_start;
+    const C ev = c < 6 ? ys[c] : t_start + dt;
+    const bool pos = c < 3 || c == 6;
+    const C scale = C(pos ? tol.pos_rtol : tol.mom_rtol) * g_max(g_abs(sv), g_abs(ev)) + C(pos ? tol.pos_atol : tol.mom_atol);
+    const C ae = g_abs(err);
+    const bool larger = ae * den > num * scale;
+    num = larger ? ae : num;
+    den = larger ? scale : den;
+    chk += err + K[6][c];
   }
   finite = g_finite(chk);
   return num * g_rcp(den);

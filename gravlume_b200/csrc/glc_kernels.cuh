@@ -140,8 +140,7 @@ struct LaunchShape {
 template <int P>
 __device__ __forceinline__ bool ray_step(Ray<P>& ray, const LaneScene& ls, const glc_policy& pol,
                                          RayResult<typename PrecTraits<P>::S>& res, bool use64) {
-  if (P == kMIXED && use64) return ray.template step<true>(ls, pol, res);
-  return ray.template step<false>(ls, pol, res);
+  return ray.step(ls, pol, res, P == kMIXED && use64);
 }
 
 // One thread per ray; rays in tile order so a warp covers a compact pixel tile.

@@ -19,6 +19,12 @@
 
 #include <type_traits>
 
+// 1: the DP5(4) attempt runs its six stages through one rolled loop (small instruction footprint);
+// 0: fully unrolled stages.
+#ifndef GLC_COMPACT_ATTEMPT
+#define GLC_COMPACT_ATTEMPT 0
+#endif
+
 #include "glc_dp54.cuh"
 #include "../../include/glc.h"
 
@@ -151,13 +157,43 @@ struct RayResult {
   S surface_r, surface_phi, g;
 };
 
+// Dense output of one step as four polynomial coefficient vectors in T (built once from the
+// stages, then evaluated by Horner's rule): y(theta) = y0 + h theta (c1 + theta (c2 + theta (c3 +
+// theta c4))).
+template <class T>
+struct DensePoly {
+  T c[4][7];
+  template <class TK>
+  GLC_HD void build(const TK K[7][7]) {
+    using namespace dp;
+    const double d[7][4] = {{d10, d11, d12, d13}, {0, 0, 0, 0},     {0, d31, d32, d33}, {0, d41, d42, d43},
+                            {0, d51, d52, d53},   {0, d61, d62, d63}, {0, d71, d72, d73}};
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int comp = 0; comp < 7; ++comp) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < 7; ++j) s += T(d[j][p]) * T(K[j][comp]);
+        c[p][comp] = s;
+      }
+  }
+  GLC_HD void eval(const T y0[6], T h, T th, T y[6], T& dt) const {
+    for (int comp = 0; comp < 7; ++comp) {
+      const T v = th * (c[0][comp] + th * (c[1][comp] + th * (c[2][comp] + th * c[3][comp])));
+      if (comp < 6) y[comp] = y0[comp] + h * v;
+      else dt = h * v;
+    }
+  }
+};
+
 // Root of an event function on the dense output between theta = 0 (value sv) and 1 (value ev).
 // The reference's oracle bisects to the affine tolerance (geodesic.rs:640-676); this is the
 // Illinois variant of regula falsi with a bisection guard, which reaches the same bracket width in
 // a handful of evaluations. Like the oracle, it stops once the bracket, in affine units, is within
 // `tol` and returns the bracket end with the smaller |value|. value_at(y, v) -> false on failure.
-template <class T, class TK, class F>
-GLC_HD bool localize(const T y0[6], T h, const TK K[7][7], T tol, T sv, T ev, F value_at, T& theta, T yroot[6],
+template <class T, class F>
+GLC_HD bool localize(const T y0[6], T h, const DensePoly<T>& K, T tol, T sv, T ev, F value_at, T& theta, T yroot[6],
                      T& bracket) {
   T lo = T(0), hi = T(1), flo = sv, fhi = ev;  // true values at the bracket ends
   T slo = sv, shi = ev;                        // Illinois-scaled values used for interpolation
@@ -180,7 +216,7 @@ GLC_HD bool localize(const T y0[6], T h, const TK K[7][7], T tol, T sv, T ev, F 
     width1 = width;
     if (mid == lo || mid == hi) break;
     T ys[6], dt;
-    dense_eval_mixed(y0, h, K, mid, ys, dt);
+    K.eval(y0, h, mid, ys, dt);
     T v;
     if (!value_at(ys, v)) return false;
     if (g_signbit(flo) == g_signbit(v)) {
@@ -202,7 +238,7 @@ GLC_HD bool localize(const T y0[6], T h, const TK K[7][7], T tol, T sv, T ev, F 
   }
   theta = g_abs(flo) <= g_abs(fhi) ? lo : hi;
   T dt;
-  dense_eval_mixed(y0, h, K, theta, yroot, dt);
+  K.eval(y0, h, theta, yroot, dt);
   bracket = (hi - lo) * ah;
   for (int c = 0; c < 6; ++c)
     if (!g_finite(yroot[c])) return false;
@@ -274,6 +310,17 @@ GLC_HD bool renormalize_null(const KN<T>& k, T y[6], T E) {
 template <int P>
 struct Ray;
 
+// Outputs of one accepted attempt that the commit and the event path need.
+template <class C>
+struct StepOutT {
+  C inc[6], k7[7];
+  C dt, r_end, vr_end, en;
+  C z0, z1;
+  Invariants<C> inv;
+  uint32_t mask;
+  bool stepped64;
+};
+
 // One binary64 DP5(4) attempt from a binary64 state (k1 evaluated at y0).
 struct Attempt64 {
   double inc[6], k7[7];
@@ -307,12 +354,11 @@ GLC_HD void attempt64(const KN<double>& kd, const double y0[6], double E, double
 #endif
 
 #if defined(__CUDA_ARCH__)
-template <int P, int K64>
+template <int P>
 __device__ __noinline__ bool rare_step_outline(Ray<P>& ray, const LaneScene& sc, const glc_policy& pol,
                                                RayResult<typename PrecTraits<P>::S>& res,
-                                               typename PrecTraits<P>::C en) {
-  using TK = typename std::conditional<K64 != 0, double, typename PrecTraits<P>::C>::type;
-  return ray.template rare_step<TK>(sc, pol, res, en);
+                                               const StepOutT<typename PrecTraits<P>::C>& o) {
+  return ray.event_path(sc, pol, res, o);
 }
 #endif
 
@@ -326,6 +372,7 @@ struct Ray {
   using S = typename PrecTraits<P>::S;
   using C = typename PrecTraits<P>::C;
   static constexpr bool kPair = P == kMIXED;
+  using StepOut = StepOutT<C>;
 
   C yh[6], yl[6];  // state (yl: MIXED low parts, zero otherwise)
   C ah, al;        // affine parameter
@@ -335,8 +382,8 @@ struct Ray {
   S az0;           // initial azimuth; the advance is az_end - az0 + 2 pi * winding
   C h;
   C k1[7];         // FSAL derivative at the state
-  S r, vr;         // event-function inputs at the state: the exact values the previous step's checks
-                   // used (kept in S, so a binary64 re-check's sign survives being stored)
+  C r, vr;         // event-function inputs at the state: the exact values the previous step's
+                   // crossing checks used as end values (the sign chain every decision follows)
   C lz0, q0, dnull, dlz, dq;
   C turn_r;
   C dir;
@@ -346,6 +393,7 @@ struct Ray {
   int32_t winding, polar;
   uint32_t flags;
   bool have_inv;
+  bool pair;       // MIXED with mixed_pair_state: compensated accumulation of state and affine
 
   GLC_HD S ys(int c) const { return kPair ? S(yh[c]) + S(yl[c]) : S(yh[c]); }
   GLC_HD void state_s(S out[6]) const {
@@ -367,6 +415,7 @@ struct Ray {
       v[3 + c] = S(st8[5 + c]);
     }
     set_state(v);
+    pair = kPair && pol.mixed_pair_state != 0u;
     E = S(-st8[4]);
     Ec = C(E);
     dir = C(direction);
@@ -386,9 +435,9 @@ struct Ray {
     C rr, vv;
     Invariants<C> inv;
     kn_rhs<C, true>(kc, yh, Ec, k1, rr, vv, &inv);
-    r = S(rr);
-    vr = S(vv);
-    if (kPair) pair_invariants(inv);
+    r = rr;
+    vr = vv;
+    if (pair) pair_invariants(inv);
     have_inv = g_finite(rr) && g_finite(inv.lz) && g_finite(inv.carter) && g_finite(inv.null_residual);
     lz0 = inv.lz;
     q0 = inv.carter;
@@ -396,8 +445,8 @@ struct Ray {
     if (have_inv) {
       dnull = inv.null_residual;
       for (int kind = 0; kind < 4; ++kind) {
-        const S vk = event_value<S>(kind, sc, pol.singularity_guard, r, v[2]);
-        if (event_clears_band(kind, vk, S(pol.event_arming_band))) armed |= 1u << kind;
+        const C vk = event_value<C>(kind, sc, pol.singularity_guard, r, yh[2]);
+        if (event_clears_band(kind, vk, C(pol.event_arming_band))) armed |= 1u << kind;
       }
     }
   }
@@ -458,19 +507,18 @@ struct Ray {
     }
   }
 
-  // Advance by one attempted step. Returns true when the ray terminated (result filled).
-  template <bool kUse64>
-  GLC_HD bool step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res) {
+  // Advance by one attempted step. Returns true when the ray terminated (result filled). use64
+  // (MIXED only): take this step in binary64 (the warp has a lane inside the shell). One step body
+  // serves both cases; only the attempt itself branches.
+  GLC_HD bool step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, bool use64) {
     if (uint64_t(accepted) >= pol.maximum_accepted_steps) {
       finish_plain(res, GLC_TERM_STEP_EXHAUSTION, GLC_FAIL_NONE);
       return true;
     }
     const Tolerance tol{pol.position_rtol, pol.position_atol, pol.momentum_rtol, pol.momentum_atol};
-    C inc[6], dt, k7[7], en;
-    S r_end, vr_end;
-    Invariants<C> inv;
+    StepOut o;
     bool finite;
-    const bool stepped64 = P == kMIXED && kUse64;
+    const bool stepped64 = P == kMIXED && use64;
     if (stepped64) {
       // binary64 step inside the shell: double k1 at the state, double stages and error control
       // (out of line on the device, so the binary32 hot loop is not register-allocated for it)
@@ -478,35 +526,33 @@ struct Ray {
       double yd[6];
       for (int c = 0; c < 6; ++c) yd[c] = double(ys(c));
       attempt64(sc.kn, yd, double(E), double(h), double(th) + double(tl), tol, &a);
-      for (int c = 0; c < 6; ++c) inc[c] = C(a.inc[c]);
-      for (int c = 0; c < 7; ++c) k7[c] = C(a.k7[c]);
-      dt = C(a.dt);
-      r_end = S(a.r_end);
-      vr_end = S(a.vr_end);
-      en = C(a.en);
+      for (int c = 0; c < 6; ++c) o.inc[c] = C(yd[c] + a.inc[c] - ys(c));
+      for (int c = 0; c < 7; ++c) o.k7[c] = C(a.k7[c]);
+      o.dt = C(a.dt);
+      o.r_end = C(a.r_end);
+      o.vr_end = C(a.vr_end);
+      o.inv.lz = C(a.inv.lz);
+      o.inv.carter = C(a.inv.carter);
+      o.inv.null_residual = C(a.inv.null_residual);
+      o.inv.abracket = C(a.inv.abracket);
+      o.en = C(a.en);
       finite = a.finite;
-      if (finite && a.en <= 1.0) {
-        // exact binary64 increments: commit them through the pair
-        if constexpr (kPair) {
-          for (int c = 0; c < 6; ++c) {
-            const double nv = yd[c] + a.inc[c];
-            inc[c] = C(nv - double(yh[c]) - double(yl[c]));
-          }
-        }
-        update_drifts(a.inv);
-      }
     } else {
       const KN<C> kc = kn_cast<C>(sc.kn);
-      C rec, vrec;
-      en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, inc, dt, k7, rec, vrec, inv, finite);
-      r_end = S(rec);
-      vr_end = S(vrec);
+#if GLC_COMPACT_ATTEMPT
+      o.en = dp5_attempt_compact<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
+                                             o.inv, finite);
+#else
+      o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
+                                     finite);
+#endif
+      if (pair) pair_invariants_after(o);
     }
-    if (!finite || !g_finite(en)) {
+    if (!finite || !g_finite(o.en)) {
       finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
       return true;
     }
-    if (en > C(1)) {
+    if (o.en > C(1)) {
       rejected += 1;
       consecutive += 1;
       if (consecutive >= pol.maximum_consecutive_rejects) {
@@ -517,7 +563,7 @@ struct Ray {
         finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_MINIMUM_STEP);
         return true;
       }
-      h = dir * next_step(pol, g_abs(h), en, false);
+      h = dir * next_step(pol, g_abs(h), o.en, false);
       return false;
     }
     accepted += 1;
@@ -526,68 +572,92 @@ struct Ray {
       f64steps += 1;
       flags |= kFlagShellF64;
     }
-    // end-of-step z (the only state component the crossing checks need)
-    C zh = yh[2], zl = yl[2];
-    if constexpr (kPair) ff_add(zh, zl, inc[2]);
-    else zh += inc[2];
-    const S z0 = ys(2), z1 = kPair ? S(zh) + S(zl) : S(zh);
-    // ---- crossing detection: start values are exactly the previous step's end values
+    // ---- crossing detection in the stepping precision; the start values are exactly the
+    // previous step's end values, so every sign change between consecutive states is seen
     const double guard = pol.singularity_guard;
-    bool any = false;
+    o.z0 = yh[2];
+    o.z1 = yh[2] + o.inc[2];
+    if (pair) {
+      C zl = yl[2], zh = yh[2];
+      ff_add_any(zh, zl, o.inc[2]);
+      o.z1 = zh;
+    }
+    uint32_t ev = 0;
     for (int kind = 0; kind < 4; ++kind) {
       if (!((armed >> kind) & 1u) || !((sc.installed >> kind) & 1u)) continue;
-      const S sv = event_value<S>(kind, sc, guard, r, z0);
-      const S evv = event_value<S>(kind, sc, guard, r_end, z1);
-      any = any || event_crosses(kind, sv, evv);
+      const C sv = event_value<C>(kind, sc, guard, r, o.z0);
+      const C evv = event_value<C>(kind, sc, guard, o.r_end, o.z1);
+      if (event_crosses(kind, sv, evv)) ev |= 1u << kind;
     }
-    const S vs = S(dir) * vr, ve = S(dir) * vr_end;
-    any = any || (vs < S(0) && ve >= S(0)) || (vs > S(0) && ve <= S(0));
-    any = any || event_crosses(kEvSurface, z0, z1);
-    if (any) {
+    const C vs = dir * vr, ve = dir * o.vr_end;
+    if ((vs < C(0) && ve >= C(0)) || (vs > C(0) && ve <= C(0))) ev |= 1u << 4;
+    if (event_crosses(kEvSurface, o.z0, o.z1)) ev |= 1u << 5;
+    o.mask = ev;
+    if (ev != 0u) {
+      o.stepped64 = stepped64;
 #if defined(__CUDA_ARCH__)
       // out-of-line event path on copies, so the hot loop keeps this ray in registers
       Ray tmp = *this;
       LaneScene lsc = sc;
       glc_policy pl = pol;
       RayResult<S> rs;
-      const bool done = rare_step_outline<P, stepped64 ? 1 : 0>(tmp, lsc, pl, rs, en);
+      const bool done = rare_step_outline<P>(tmp, lsc, pl, rs, o);
       *this = tmp;
       if (done) res = rs;
-      return done;
+      if (done) return true;
 #else
-      if (stepped64) return rare_step<double>(sc, pol, res, en);
-      return rare_step<C>(sc, pol, res, en);
+      if (event_path(sc, pol, res, o)) return true;
 #endif
     }
-    // ---- plain commit
+    commit(sc, pol, o, stepped64);
+    return false;
+  }
+
+  // Plain commit of an accepted, non-terminal step.
+  GLC_HD void commit(const LaneScene& sc, const glc_policy& pol, const StepOut& o, bool stepped64) {
     const C x_old = yh[0], y_old = yh[1];
-    add_time(dt);
-    if constexpr (kPair) {
-      for (int c = 0; c < 6; ++c) ff_add(yh[c], yl[c], inc[c]);
-      ff_add(ah, al, h);
+    add_time(o.dt);
+    if (pair) {
+      for (int c = 0; c < 6; ++c) ff_add_any(yh[c], yl[c], o.inc[c]);
+      ff_add_any(ah, al, h);
     } else {
-      for (int c = 0; c < 6; ++c) yh[c] += inc[c];
+      for (int c = 0; c < 6; ++c) yh[c] += o.inc[c];
       ah += h;
     }
     commit_azimuth(S(x_old), S(y_old), S(yh[0]), S(yh[1]));
-    if (!stepped64) {
-      if (kPair) pair_invariants(inv);
-      update_drifts(inv);
-    }
-    for (int c = 0; c < 7; ++c) k1[c] = k7[c];
-    r = r_end;
-    vr = vr_end;
+    update_drifts(o.inv);
+    for (int c = 0; c < 7; ++c) k1[c] = o.k7[c];
+    r = o.r_end;
+    vr = o.vr_end;
     arm_update(sc, pol);
-    h = dir * next_step(pol, g_abs(h), en, true);
-    return false;
+    h = dir * next_step(pol, g_abs(h), o.en, true);
+    (void)stepped64;
+  }
+
+  GLC_HD void pair_invariants_after(StepOut& o) const {
+    if constexpr (kPair) {
+      // L from the end-of-step pair state (compensated products)
+      C hh[6], ll[6];
+      for (int c = 0; c < 6; ++c) {
+        hh[c] = yh[c];
+        ll[c] = yl[c];
+        ff_add_any(hh[c], ll[c], o.inc[c]);
+      }
+      const float lx = ff_cross(hh[1], ll[1], hh[5], ll[5], hh[2], ll[2], hh[4], ll[4]);
+      const float ly = ff_cross(hh[2], ll[2], hh[3], ll[3], hh[0], ll[0], hh[5], ll[5]);
+      o.inv.lz = ff_cross(hh[0], ll[0], hh[4], ll[4], hh[1], ll[1], hh[3], ll[3]);
+      o.inv.carter = lx * lx + ly * ly + o.inv.abracket;
+    } else {
+      (void)o;
+    }
   }
 
   GLC_HD void arm_update(const LaneScene& sc, const glc_policy& pol) {
     if (armed == 0xFu) return;
     for (int kind = 0; kind < 4; ++kind) {
       if ((armed >> kind) & 1u) continue;
-      const S v = event_value<S>(kind, sc, pol.singularity_guard, r, ys(2));
-      if (event_clears_band(kind, v, S(pol.event_arming_band))) armed |= 1u << kind;
+      const C v = event_value<C>(kind, sc, pol.singularity_guard, r, yh[2]);
+      if (event_clears_band(kind, v, C(pol.event_arming_band))) armed |= 1u << kind;
     }
   }
 
@@ -602,70 +672,58 @@ struct Ray {
     if (kPair) ff_add_any(ah, al, C(v - S(hi)));
   }
 
-  // Event path in precision S (binary64 in MIXED): recompute the stages for dense output, then
-  // localize events, turning points and equatorial crossings and commit. The sign tests use the
-  // stored start values (r, vr: what the previous step's end checks used), so a crossing is never
-  // lost between a binary32 detection and a binary64 re-check.
-  // TK is the stage precision of the event path: the stepping precision (binary32 in MIXED
-  // outside the shell, binary64 on shell steps); the dense state, the event functions and the
-  // committed state are in S.
-  template <class TK>
-  GLC_HD bool rare_step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, C en) {
+  // Event path of an accepted step with a sign change (o.mask: bits 0-3 events, 4 radial turning,
+  // 5 equator). The decisions are the stepping-precision sign tests already taken; here the roots
+  // are localized on the step's dense output in precision S (binary64 in MIXED: a binary64 dense
+  // polynomial from the stepping-precision stages), events are ordered and, for a terminal event,
+  // the observables are evaluated in S. Returns true when the ray terminated; otherwise the caller
+  // commits the step as a plain one.
+  GLC_HD bool event_path(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, const StepOut& o) {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
-    const KN<TK> kk = kn_cast<TK>(sc.kn);
-    TK K[7][7];
     T y[6];
     state_s(y);
-    TK yk[6];
-    for (int c = 0; c < 6; ++c) yk[c] = TK(y[c]);
-    {
-      TK rr, vv;
-      if (P == kMIXED && sizeof(TK) == sizeof(double)) {
-        kn_rhs(kk, yk, TK(E), K[0], rr, vv);  // shell step: binary64 k1
-      } else {
-        for (int c = 0; c < 7; ++c) K[0][c] = TK(k1[c]);
-      }
+    // stages for the dense output, in the stepping precision (binary64 on MIXED shell steps)
+    DensePoly<T> dpoly;
+    if (o.stepped64) {
+      double K[7][7], yk[6], rr, vv, ye[6];
+      for (int c = 0; c < 6; ++c) yk[c] = double(y[c]);
+      kn_rhs(sc.kn, yk, double(E), K[0], rr, vv);
+      dp5_stages(sc.kn, yk, double(E), double(h), K, ye, rr, vv);
+      dpoly.build(K);
+    } else {
+      const KN<C> kc = kn_cast<C>(sc.kn);
+      C K[7][7], ye[6], rr, vv;
+      for (int c = 0; c < 7; ++c) K[0][c] = k1[c];
+      dp5_stages(kc, yh, Ec, h, K, ye, rr, vv);
+      dpoly.build(K);
     }
-    const T r0 = T(r), vr0 = T(vr);
     const T hh = T(h);
-    TK yend_k[6], rk, vrk;
-    dp5_stages(kk, yk, TK(E), TK(h), K, yend_k, rk, vrk);
-    T yend[6], r_end;
-    {
-      T dtd;
-      dense_eval_mixed(y, hh, K, T(1), yend, dtd);
-      int gs;
-      r_end = sizeof(TK) == sizeof(T) ? T(rk) : kn_radius(kt, yend[0], yend[1], yend[2], gs);
-    }
-    const T vr_end = T(vrk);
     const double guard = pol.singularity_guard;
     const T tol = T(pol.event_affine_tolerance);
-    bool fail = false;
     int n = 0;
     int kinds[4];
     T thetas[4], residuals[4], states[4][6];
     for (int kind = 0; kind < 4; ++kind) {
-      if (!((armed >> kind) & 1u) || !((sc.installed >> kind) & 1u)) continue;
-      const T sv = event_value<T>(kind, sc, guard, r0, y[2]);
-      const T evv = event_value<T>(kind, sc, guard, r_end, yend[2]);
-      if (!event_crosses(kind, sv, evv)) continue;
-      T th, yr[6], br;
-      auto value_at = [&](const T* ys, T& v) -> bool {
+      if (!((o.mask >> kind) & 1u)) continue;
+      const T sv = T(event_value<C>(kind, sc, guard, r, o.z0));
+      const T evv = T(event_value<C>(kind, sc, guard, o.r_end, o.z1));
+      T th_, yr[6], br;
+      auto value_at = [&](const T* ys_, T& v) -> bool {
         int gs = kGeomOk;
-        const T rr = kind == kEvSurface ? T(0) : kn_radius(kt, ys[0], ys[1], ys[2], gs);
+        const T rr = kind == kEvSurface ? T(0) : kn_radius(kt, ys_[0], ys_[1], ys_[2], gs);
         if (gs != kGeomOk) return false;
-        v = event_value<T>(kind, sc, guard, rr, ys[2]);
+        v = event_value<T>(kind, sc, guard, rr, ys_[2]);
         return true;
       };
-      if (!localize(y, hh, K, tol, sv, evv, value_at, th, yr, br)) {
-        fail = true;
-        break;
+      if (!localize(y, hh, dpoly, tol, sv, evv, value_at, th_, yr, br)) {
+        finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
+        return true;
       }
       T rv;
       if (!value_at(yr, rv)) {
-        fail = true;
-        break;
+        finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
+        return true;
       }
       bool keep = true;
       if (kind == kEvSurface) {
@@ -675,15 +733,11 @@ struct Ray {
       }
       if (keep) {
         kinds[n] = kind;
-        thetas[n] = th;
+        thetas[n] = th_;
         residuals[n] = g_abs(rv) / T(event_scale(kind, sc));
         for (int c = 0; c < 6; ++c) states[n][c] = yr[c];
         ++n;
       }
-    }
-    if (fail) {
-      finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
-      return true;
     }
     int first = -1;
     uint32_t cand = 0;
@@ -695,42 +749,42 @@ struct Ray {
     const bool has_event = first >= 0;
     const T term_theta = has_event ? thetas[first] : T(1);
     // radial turning point (geodesic.rs:330-360)
-    {
-      const T sv = T(dir) * vr0, evv = T(dir) * vr_end;
-      if ((sv < T(0) && evv >= T(0)) || (sv > T(0) && evv <= T(0))) {
-        T th, yr[6], br;
-        auto vr_at = [&](const T* ys, T& v) -> bool {
-          TK d[7], rr, vv, yy[6];
-          for (int c = 0; c < 6; ++c) yy[c] = TK(ys[c]);
-          kn_rhs(kk, yy, TK(E), d, rr, vv);
-          v = T(dir) * T(vv);
-          return g_finite(v);
-        };
-        if (localize(y, hh, K, tol, sv, evv, vr_at, th, yr, br) && (!has_event || th < term_theta)) {
-          turnings += 1;
-          if (sv < T(0) && evv >= T(0)) {
-            int gs;
-            const T rr = kn_radius(kt, yr[0], yr[1], yr[2], gs);
-            if (gs == kGeomOk) turn_r = (turn_r == turn_r) ? C(g_min(T(turn_r), rr)) : C(rr);
-          }
+    if ((o.mask >> 4) & 1u) {
+      const T sv = T(dir * vr), evv = T(dir * o.vr_end);
+      T th_, yr[6], br;
+      auto vr_at = [&](const T* ys_, T& v) -> bool {
+        C d[7], rr, vv, yy[6];
+        for (int c = 0; c < 6; ++c) yy[c] = C(ys_[c]);
+        kn_rhs(kn_cast<C>(sc.kn), yy, Ec, d, rr, vv);
+        v = T(dir * vv);
+        return g_finite(v);
+      };
+      if (localize(y, hh, dpoly, tol, sv, evv, vr_at, th_, yr, br) && (!has_event || th_ < term_theta)) {
+        turnings += 1;
+        if (sv < T(0) && evv >= T(0)) {
+          int gs;
+          const T rr = kn_radius(kt, yr[0], yr[1], yr[2], gs);
+          if (gs == kGeomOk) turn_r = (turn_r == turn_r) ? C(g_min(T(turn_r), rr)) : C(rr);
         }
       }
     }
     // equatorial crossing (geodesic.rs:362-383)
-    if (event_crosses(kEvSurface, y[2], yend[2])) {
-      T th, yr[6], br;
-      auto z_at = [&](const T* ys, T& v) -> bool {
-        v = ys[2];
+    if ((o.mask >> 5) & 1u) {
+      T th_, yr[6], br;
+      auto z_at = [&](const T* ys_, T& v) -> bool {
+        v = ys_[2];
         return true;
       };
-      if (localize(y, hh, K, tol, y[2], yend[2], z_at, th, yr, br) && (!has_event || th < term_theta)) crossings += 1;
+      if (localize(y, hh, dpoly, tol, T(o.z0), T(o.z1), z_at, th_, yr, br) && (!has_event || th_ < term_theta))
+        crossings += 1;
     }
-    // commit at the terminal theta (or the step end)
+    if (!has_event) return false;
+    // terminal commit at the event (precision S)
     T ycommit[6], dtc;
     {
       T ytmp[6];
-      dense_eval_mixed(y, hh, K, term_theta, ytmp, dtc);
-      for (int c = 0; c < 6; ++c) ycommit[c] = has_event ? states[first][c] : yend[c];
+      dpoly.eval(y, hh, term_theta, ytmp, dtc);
+      for (int c = 0; c < 6; ++c) ycommit[c] = states[first][c];
     }
     add_time_s(dtc);
     commit_azimuth(y[0], y[1], ycommit[0], ycommit[1]);
@@ -739,25 +793,15 @@ struct Ray {
       const T rr = kn_radius(kt, ycommit[0], ycommit[1], ycommit[2], gs);
       if (gs == kGeomOk) update_drifts(kn_invariants(kt, ycommit, E, rr));
     }
-    if (has_event) {
-      add_affine_s(hh * term_theta);
-      set_state(ycommit);
-      const int kind = kinds[first];
-      uint32_t term = GLC_TERM_HORIZON;
-      if (kind == kEvGuard) term = GLC_TERM_SINGULARITY;
-      else if (kind == kEvSurface) term = GLC_TERM_SURFACE;
-      else if (kind == kEvEscape) term = GLC_TERM_ESCAPE;
-      finish_event(sc, pol, res, term, cand, residuals[first]);
-      return true;
-    }
-    add_affine_s(hh);
-    set_state(yend);
-    for (int c = 0; c < 7; ++c) k1[c] = C(K[6][c]);
-    r = r_end;
-    vr = vr_end;
-    arm_update(sc, pol);
-    h = dir * next_step(pol, g_abs(h), en, true);
-    return false;
+    add_affine_s(hh * term_theta);
+    set_state(ycommit);
+    const int kind = kinds[first];
+    uint32_t term = GLC_TERM_HORIZON;
+    if (kind == kEvGuard) term = GLC_TERM_SINGULARITY;
+    else if (kind == kEvSurface) term = GLC_TERM_SURFACE;
+    else if (kind == kEvEscape) term = GLC_TERM_ESCAPE;
+    finish_event(sc, pol, res, term, cand, residuals[first], ycommit);
+    return true;
   }
 
   GLC_HD void finish_plain(RayResult<S>& res, uint32_t term, uint32_t failure) {
@@ -772,11 +816,11 @@ struct Ray {
 
   // Terminal observables at the committed event state y (precision S; binary64 in MIXED).
   GLC_HD void finish_event(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, uint32_t term,
-                           uint32_t cand, S residual) {
+                           uint32_t cand, S residual, const S ystate[6]) {
     using T = S;
     const KN<T> kt = kn_cast<T>(sc.kn);
     T ye[6];
-    state_s(ye);
+    for (int c = 0; c < 6; ++c) ye[c] = ystate[c];
     if (P == kMIXED && pol.renormalize_null) {
       if (renormalize_null(kt, ye, E)) flags |= kFlagRenormalized;
     }

@@ -140,7 +140,7 @@ typedef struct glc_policy {
   uint32_t refill_interval;       /* persistent: steps between warp refills of finished lanes */
   uint32_t rays_per_grab;         /* persistent: rays a warp takes from the queue per refill (>= 32) */
   uint32_t refill_min_idle;       /* persistent: idle lanes that trigger a refill (1..32) */
-  uint32_t reserved_policy;
+  uint32_t mixed_pair_state;      /* MIXED: accumulate the state as compensated binary32 pairs */
 } glc_policy;
 
 typedef enum glc_camera_kind {

@@ -19,7 +19,7 @@ void run(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st
     RayResult<typename PrecTraits<P>::S> res;
     for (;;) {
       const bool use64 = P == kMIXED && double(ray.r) < ls.shell_r;
-      const bool done = use64 ? ray.template step<true>(ls, pol, res) : ray.template step<false>(ls, pol, res);
+      const bool done = ray.step(ls, pol, res, use64);
       if (done) break;
     }
     double* o = out + nf * i;
