@@ -116,6 +116,8 @@ SIGNATURES = {
     "glc_graph_destroy": (c_int32, [c_void_p]),
     "glc_autotune": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_int32,
                                ctypes.POINTER(Results), c_void_p, c_int32, ctypes.POINTER(Policy)]),
+    "glc_trace_static_scratch": (c_int32, [c_void_p, c_int32, c_void_p, c_int32, ctypes.POINTER(Policy),
+                                           ctypes.POINTER(Results), c_void_p]),
 }
 
 _lib = None

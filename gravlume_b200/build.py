@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB_PATH = LIB_DIR / "libglc.so"
 
-SOURCES = ["glc_api.cu", "glc_scene.cpp", "glc_flops.cpp"]
+SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_scene.cpp", "glc_flops.cpp"]
 HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_internal.h"]
 
 NVCC_FLAGS = [

@@ -256,6 +256,19 @@ glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
                         int32_t n_cameras, const glc_results* out, void* stream, int32_t repeats,
                         glc_policy* policy);
 
+/* ---- trace without device allocation ------------------------------------------------------ */
+/* No counterpart in the reference: its wgpu trace pass always allocates its own target and
+ * scratch. For callers that may not allocate device memory (a host whose frame allocator owns the
+ * device heap, a plugin confined to buffers its host hands it): the persistent work-queue trace of
+ * glc_trace, without a context. Its scratch (queue counter and job table) is a 64 KiB static
+ * device array, so at most 128 scenes and 128 cameras (GLC_ERR_CAPACITY beyond). Runs on the
+ * current device; the first call on a device looks up the array's address, so make it before any
+ * stream capture. All calls share the array: calls that overlap on the GPU race. Scenes, cameras
+ * and policy are host structs; results (and RAYLIST states) are device pointers. */
+glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                                    int32_t n_cameras, const glc_policy* policy, const glc_results* out,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif
