@@ -18,7 +18,8 @@ LIB_DIR = PKG / "_lib"
 LIB_PATH = LIB_DIR / "libglc.so"
 
 SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_scene.cpp", "glc_flops.cpp"]
-HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_internal.h"]
+HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh",
+           "glc_internal.h"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

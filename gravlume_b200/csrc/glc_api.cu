@@ -10,7 +10,7 @@
 #include <vector>
 
 #include "glc_internal.h"
-#include "glc_kernels.cuh"
+#include "glc_certificate.cuh"
 
 using namespace glc;
 
@@ -54,8 +54,9 @@ size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 // Host-side description of a job: padded ray counts per camera and the device-table layout.
 struct JobLayout {
   std::vector<unsigned long long> begin;
+  std::vector<unsigned long long> cert_begin;  // 16x16 certificate tiles of each image camera
   unsigned long long total = 0;
-  size_t off_scenes = 0, off_cams = 0, off_begin = 0, bytes = 0;
+  size_t off_scenes = 0, off_cams = 0, off_begin = 0, off_cert_begin = 0, bytes = 0;
 };
 
 glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cams, int32_t n_cams,
@@ -64,7 +65,8 @@ glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_cam
     return set_error(GLC_ERR_INVALID_ARGUMENT, "scenes and cameras must be non-empty");
   if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
   L.begin.assign(size_t(n_cams) + 1, 0);
-  unsigned long long acc = 0;
+  L.cert_begin.assign(size_t(n_cams) + 1, 0);
+  unsigned long long acc = 0, tiles = 0;
   for (int i = 0; i < n_cams; ++i) {
     const glc_camera& c = cams[i];
     if (c.scene_index < 0 || c.scene_index >= n_scenes)
@@ -92,13 +94,18 @@ glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_cam
     }
     L.begin[i] = acc;
     acc += n;
+    L.cert_begin[i] = tiles;
+    if (c.kind != GLC_CAMERA_RAYLIST)
+      tiles += (unsigned long long)((c.width + kCertTile - 1) / kCertTile) * ((c.height + kCertTile - 1) / kCertTile);
   }
   L.begin[n_cams] = acc;
+  L.cert_begin[n_cams] = tiles;
   L.total = acc;
   L.off_scenes = 0;
   L.off_cams = align256(sizeof(glc_scene) * n_scenes);
   L.off_begin = L.off_cams + align256(sizeof(glc_camera) * n_cams);
-  L.bytes = L.off_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
+  L.off_cert_begin = L.off_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
+  L.bytes = L.off_cert_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
   return GLC_OK;
 }
 
@@ -107,6 +114,7 @@ void fill_staging(unsigned char* stage, const JobLayout& L, const glc_scene* sce
   std::memcpy(stage + L.off_scenes, scenes, sizeof(glc_scene) * n_scenes);
   std::memcpy(stage + L.off_cams, cams, sizeof(glc_camera) * n_cams);
   std::memcpy(stage + L.off_begin, L.begin.data(), sizeof(unsigned long long) * (n_cams + 1));
+  std::memcpy(stage + L.off_cert_begin, L.cert_begin.data(), sizeof(unsigned long long) * (n_cams + 1));
 }
 
 JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
@@ -116,6 +124,8 @@ JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
   v.begin = reinterpret_cast<const unsigned long long*>(dev + L.off_begin);
   v.n_cams = n_cams;
   v.total = L.total;
+  v.cert_begin = reinterpret_cast<const unsigned long long*>(dev + L.off_cert_begin);
+  v.cert = nullptr;
   return v;
 }
 
@@ -132,6 +142,8 @@ struct glc_ctx {
   cudaEvent_t stage_free = nullptr;  // recorded after the last staging copy
   bool stage_pending = false;
   unsigned long long* d_queue = nullptr;
+  uint32_t* d_cert = nullptr;          // per-tile capture certificates (grow-only)
+  size_t d_cert_words = 0;
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
   size_t d_host_ws_bytes = 0;
   glc_launch_stats stats{};
@@ -144,6 +156,7 @@ struct glc_graph {
   unsigned char* d_job = nullptr;
   unsigned char* h_stage = nullptr;
   unsigned long long* d_queue = nullptr;
+  uint32_t* d_cert = nullptr;
 };
 
 namespace {
@@ -180,17 +193,37 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
   return GLC_OK;
 }
 
-glc_status launch(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out, cudaStream_t stream,
-                  unsigned long long* queue) {
-  if (job.total == 0) return GLC_OK;
+// cert: device words for the job's certificate tiles (at least cert_tiles of them) when the policy
+// asks for certificates, else unused.
+glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, const glc_results& out,
+                  cudaStream_t stream, unsigned long long* queue, uint32_t* cert = nullptr,
+                  unsigned long long cert_tiles = 0) {
+  if (job_in.total == 0) return GLC_OK;
   if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
     return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
+  JobView job = job_in;
+  if (pol.capture_certificates && cert && cert_tiles > 0) {
+    certify_tiles_kernel<<<unsigned((cert_tiles + 127) / 128), 128, 0, stream>>>(job, cert);
+    GLC_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+    job.cert = cert;
+  }
   switch (pol.precision) {
     case GLC_FP32: return launch_precision<kFP32>(ctx, job, pol, out, stream, queue);
     case GLC_MIXED: return launch_precision<kMIXED>(ctx, job, pol, out, stream, queue);
     case GLC_FP64: return launch_precision<kFP64>(ctx, job, pol, out, stream, queue);
     default: return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown precision mode");
   }
+}
+
+glc_status ensure_cert_capacity(uint32_t** buf, size_t* words, unsigned long long need) {
+  if (need <= *words) return GLC_OK;
+  if (*buf) GLC_CUDA(cudaFree(*buf));
+  *buf = nullptr;
+  *words = 0;
+  GLC_CUDA(cudaMalloc(buf, need * sizeof(uint32_t)));
+  *words = need;
+  return GLC_OK;
 }
 
 glc_status validate_policy(const glc_policy& p) {
@@ -338,6 +371,7 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
   p.rays_per_grab = 64;
   p.refill_min_idle = 16;
   p.mixed_pair_state = 0;
+  p.capture_certificates = 0;
   *out = p;
   return GLC_OK;
 }
@@ -401,6 +435,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_job) cudaFree(ctx->d_job);
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->d_queue) cudaFree(ctx->d_queue);
+  if (ctx->d_cert) cudaFree(ctx->d_cert);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
@@ -456,7 +491,12 @@ glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, co
   GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, st));
   GLC_CUDA(cudaEventRecord(ctx->stage_free, st));
   ctx->stage_pending = true;
-  return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue);
+  const unsigned long long tiles = ctx->policy.capture_certificates ? L.cert_begin[n_cameras] : 0ull;
+  if (tiles) {
+    s = ensure_cert_capacity(&ctx->d_cert, &ctx->d_cert_words, tiles);
+    if (s != GLC_OK) return s;
+  }
+  return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue, ctx->d_cert, tiles);
 }
 
 glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
@@ -530,18 +570,22 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
     if (G->d_job) cudaFree(G->d_job);
     if (G->h_stage) cudaFreeHost(G->h_stage);
     if (G->d_queue) cudaFree(G->d_queue);
+    if (G->d_cert) cudaFree(G->d_cert);
     delete G;
     return st;
   };
+  const unsigned long long tiles = ctx->policy.capture_certificates ? L.cert_begin[n_cameras] : 0ull;
   if (cudaMalloc(&G->d_job, L.bytes) != cudaSuccess || cudaMallocHost(&G->h_stage, L.bytes) != cudaSuccess ||
-      cudaMalloc(&G->d_queue, 256) != cudaSuccess)
+      cudaMalloc(&G->d_queue, 256) != cudaSuccess ||
+      (tiles && cudaMalloc(&G->d_cert, tiles * sizeof(uint32_t)) != cudaSuccess))
     return fail(set_error(GLC_ERR_CUDA, "graph buffer allocation failed"));
   fill_staging(G->h_stage, L, scenes, n_scenes, cameras, n_cameras);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return fail(set_error(GLC_ERR_CUDA, "cudaStreamBeginCapture failed"));
   cudaError_t ce = cudaMemcpyAsync(G->d_job, G->h_stage, L.bytes, cudaMemcpyHostToDevice, st);
-  glc_status ls = ce == cudaSuccess ? launch(ctx, job_view(G->d_job, L, n_cameras), ctx->policy, *out, st, G->d_queue)
+  glc_status ls = ce == cudaSuccess ? launch(ctx, job_view(G->d_job, L, n_cameras), ctx->policy, *out, st, G->d_queue,
+                                           G->d_cert, tiles)
                                     : set_error(GLC_ERR_CUDA, cudaGetErrorString(ce));
   cudaGraph_t gr = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(st, &gr);
@@ -574,6 +618,7 @@ glc_status glc_graph_destroy(glc_graph* graph) {
   if (graph->d_job) cudaFree(graph->d_job);
   if (graph->h_stage) cudaFreeHost(graph->h_stage);
   if (graph->d_queue) cudaFree(graph->d_queue);
+  if (graph->d_cert) cudaFree(graph->d_cert);
   delete graph;
   return GLC_OK;
 }

@@ -15,6 +15,8 @@ struct JobView {
   const unsigned long long* begin;  // n_cams + 1 entries
   int n_cams;
   unsigned long long total;
+  const unsigned long long* cert_begin;  // n_cams + 1 entries: first 16x16-tile word of each camera
+  const uint32_t* cert;                  // per-tile capture certificates, or null when not evaluated
 };
 
 // Initial state of ray gi of the job. Image rays are generated in binary64 from the camera basis
@@ -22,7 +24,9 @@ struct JobView {
 // p^mu = omega (u^mu - sight^mu), p_mu = g_{mu nu} p^nu at the observer. Returns false for tile
 // padding outside the image.
 __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& pol, unsigned long long gi,
-                                          double st8[8], double& dir, unsigned long long& slot, int& scene_idx) {
+                                          double st8[8], double& dir, unsigned long long& slot, int& scene_idx,
+                                          bool& certified) {
+  certified = false;
   int lo = 0, hi = job.n_cams - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -55,6 +59,13 @@ __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& 
   if (px >= W || py >= H) return false;
   slot = cam->result_offset + (unsigned long long)py * W + px;
   dir = -1.0;
+  if (job.cert) {
+    const unsigned long long t = job.cert_begin[lo] + (unsigned long long)(py >> 4) * ((W + 15u) >> 4) + (px >> 4);
+    if (job.cert[t]) {
+      certified = true;
+      return true;
+    }
+  }
   const glc_scene* sc = job.scenes + scene_idx;
   double sight[4];
   if (cam->kind == GLC_CAMERA_PINHOLE) {
@@ -120,6 +131,25 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
   }
 }
 
+// A ray of a certified tile: horizon capture proven without integration (flag bit 2, code bit
+// 22); the integration observables are NaN and the counters zero.
+__device__ __forceinline__ void write_certified(const glc_results& o, unsigned long long slot) {
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  const uint32_t code = uint32_t(GLC_TERM_HORIZON) | (1u << 16) | (4u << 20);
+  if (o.code) reinterpret_cast<uint4*>(o.code)[slot] = make_uint4(code, 0u, 0u, 0u);
+  if (o.branch) reinterpret_cast<int4*>(o.branch)[slot] = make_int4(0, 0, 0, 0);
+  const double2 nn = make_double2(nan, nan);
+  if (o.escape) reinterpret_cast<double2*>(o.escape)[slot] = nn;
+  if (o.surface) reinterpret_cast<double2*>(o.surface)[slot] = nn;
+  if (o.redshift_time) reinterpret_cast<double2*>(o.redshift_time)[slot] = nn;
+  if (o.event) reinterpret_cast<double2*>(o.event)[slot] = nn;
+  if (o.drift_a) reinterpret_cast<double2*>(o.drift_a)[slot] = make_double2(0.0, 0.0);
+  if (o.drift_b) reinterpret_cast<double2*>(o.drift_b)[slot] = make_double2(0.0, 0.0);
+  if (o.turning) reinterpret_cast<double2*>(o.turning)[slot] = nn;
+  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = nn;
+  if (o.position_zr) reinterpret_cast<double2*>(o.position_zr)[slot] = nn;
+}
+
 // Register budget per precision: binary32 fits 128 registers (16 warps per SM); the binary64 and
 // mixed kernels carry binary64 event and shell paths and run at 2 blocks of 128 threads per SM.
 #ifndef GLC_MIN_BLOCKS_FP32
@@ -152,7 +182,12 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_
   double st8[8], dir;
   unsigned long long slot;
   int scene_idx;
-  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx)) return;
+  bool certified;
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified)) return;
+  if (certified) {
+    write_certified(out, slot);
+    return;
+  }
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
   Ray<P> ray;
   ray.init(ls, pol, st8, dir);
@@ -213,10 +248,15 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
         if (mine) {
           double st8[8], dir;
           int scene_idx;
-          if (ray_setup(job, pol, grab_next + rank, st8, dir, slot, scene_idx)) {
-            ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
-            ray.init(ls, pol, st8, dir);
-            active = true;
+          bool certified;
+          if (ray_setup(job, pol, grab_next + rank, st8, dir, slot, scene_idx, certified)) {
+            if (certified) {
+              write_certified(out, slot);
+            } else {
+              ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
+              ray.init(ls, pol, st8, dir);
+              active = true;
+            }
           }
         }
         const unsigned took = __ballot_sync(FULL, mine);

@@ -141,6 +141,8 @@ typedef struct glc_policy {
   uint32_t rays_per_grab;         /* persistent: rays a warp takes from the queue per refill (>= 32) */
   uint32_t refill_min_idle;       /* persistent: idle lanes that trigger a refill (1..32) */
   uint32_t mixed_pair_state;      /* MIXED: accumulate the state as compensated binary32 pairs */
+  uint32_t capture_certificates;  /* 1: interval capture certificates on 16x16 tiles of image
+                                     cameras of surface-free scenes; certified rays skip integration */
 } glc_policy;
 
 typedef enum glc_camera_kind {
@@ -163,7 +165,8 @@ typedef struct glc_camera {
 /* Caller-owned device SoA, one 16-byte element per ray in each array (128-bit stores). Any
  * pointer may be NULL to skip that field. Lengths: >= max(result_offset + rays of camera).
  *   code.x  termination | failure << 8 | event candidates << 12 | (polar side + 1) << 16
- *           | flags << 20 (bit 20: shell steps taken in binary64; bit 21: null renormalized)
+ *           | flags << 20 (bit 20: shell steps taken in binary64; bit 21: null renormalized;
+ *           bit 22: capture proven by the tile's interval certificate, ray not integrated)
  *   code.y  accepted steps, code.z rejected steps, code.w binary64 steps (MIXED)
  *   branch  radial turnings, equatorial crossings, azimuth winding, has turning radius
  *   escape  (polar angle, azimuth) of the unit coordinate direction at escape (NaN otherwise)

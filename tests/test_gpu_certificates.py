@@ -1,0 +1,102 @@
+"""Interval capture certificates on 16x16 tiles (crates/gravlume-render/src/shaders/
+geodesic_acceleration.wgsl:115-279, evaluated per tile with directed rounding).
+
+Soundness is checked against full integration: every ray of a certified tile must be a horizon
+capture when the same frame is integrated without certificates (binary64 kernel) and when the
+binary64 oracle traces it. Usefulness: a fair share of the shadow must be certified.
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import gravlume_b200 as G
+from gravlume_b200 import _native as N
+import oracle as O
+from gpu_common import config1_observation, oracle_for
+
+pytestmark = pytest.mark.gpu
+
+CERTIFIED = 4  # bit 22 of code.x, i.e. bit 2 of the decoded flags
+
+
+@pytest.fixture(scope="module")
+def pipe():
+    p = G.TracePipeline(0)
+    yield p
+    p.close()
+
+
+def run(pipe, scenes, cams, slots, certificates, precision=G.Precision.FP64):
+    pipe.set_policy(G.ReferencePolicy.frame(precision, capture_certificates=int(certificates)))
+    res = G.TraceResults(slots, "cuda")
+    pipe.trace(scenes, cams, res)
+    torch.cuda.synchronize()
+    return res.numpy()
+
+
+def sky_observation(width, height, radius=50.0, incl=75.0):
+    return config1_observation(width=width, height=height, r_obs=radius, incl_deg=incl, surface=False)
+
+
+@pytest.mark.parametrize("precision", [G.Precision.FP64, G.Precision.MIXED, G.Precision.FP32])
+def test_certified_pinhole_tiles_are_captured_by_full_integration(pipe, precision):
+    obs = sky_observation(768, 768)
+    sc = obs.pack()
+    cams = [G.image_camera(0, 768, 768)]
+    on = run(pipe, [sc], cams, 768 * 768, True, precision)
+    off = run(pipe, [sc], cams, 768 * 768, False, G.Precision.FP64)
+    cert = (on["flags"] & CERTIFIED) != 0
+    horizon = off["termination"] == G.Termination.HORIZON_CROSSING
+    print(precision.name, "certified", int(cert.sum()), "horizon", int(horizon.sum()))
+    assert cert.any()
+    assert np.all(on["termination"][cert] == G.Termination.HORIZON_CROSSING)
+    assert np.all(horizon[cert]), "a certified ray escaped or hit something under full integration"
+    assert cert.sum() >= 0.4 * horizon.sum()
+    assert np.all(on["accepted_steps"][cert] == 0)
+    # certified tiles are whole 16x16 tiles
+    c2 = cert.reshape(768, 768)
+    for ty in range(0, 768, 16):
+        for tx in range(0, 768, 16):
+            blk = c2[ty:ty + 16, tx:tx + 16]
+            assert blk.all() or not blk.any()
+    # uncertified rays are integrated exactly as without certificates
+    if precision == G.Precision.FP64:
+        for k in ("termination", "accepted_steps", "rejected_steps"):
+            np.testing.assert_array_equal(on[k][~cert], off[k][~cert])
+
+
+def test_certified_rays_are_captured_by_the_oracle(pipe):
+    obs = sky_observation(512, 512)
+    sc = obs.pack()
+    on = run(pipe, [sc], [G.image_camera(0, 512, 512)], 512 * 512, True)
+    idx = np.flatnonzero(on["flags"] & CERTIFIED)
+    assert idx.size > 0
+    rng = np.random.default_rng(7)
+    pick = np.sort(rng.choice(idx, size=min(64, idx.size), replace=False))
+    osc, ev, _ = oracle_for(obs)
+    ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, pick % 512, pick // 512,
+                                 threads=O.hardware_threads())
+    assert (status == 0).all()
+    assert np.all(ref[:, O.F["termination"]].astype(int) == G.Termination.HORIZON_CROSSING)
+
+
+def test_equirect_escape_map_certificates(pipe):
+    obs = sky_observation(64, 64, radius=15.0, incl=75.0)
+    sc = obs.pack()
+    cam = G.image_camera(0, 2048, 1024, kind=N.CAMERA_EQUIRECT)
+    on = run(pipe, [sc], [cam], 2048 * 1024, True)
+    off = run(pipe, [sc], [cam], 2048 * 1024, False)
+    cert = (on["flags"] & CERTIFIED) != 0
+    horizon = off["termination"] == G.Termination.HORIZON_CROSSING
+    print("equirect certified", int(cert.sum()), "horizon", int(horizon.sum()))
+    assert cert.any()
+    assert np.all(horizon[cert])
+
+
+def test_scenes_with_a_surface_are_never_certified(pipe):
+    obs = config1_observation(width=256, height=256)
+    on = run(pipe, [obs.pack()], [G.image_camera(0, 256, 256)], 256 * 256, True)
+    assert not np.any(on["flags"] & CERTIFIED)
