@@ -10,5 +10,5 @@ from ._native import GlcError, lib  # noqa: F401
 from .build import LIB_PATH, build  # noqa: F401
 from .trace import (  # noqa: F401
     EquatorialSurface, Graph, KerrSchildChart, Observation, Precision, ReferencePolicy, Termination,
-    TracePipeline, TraceResults, image_camera, oblate_to_cartesian, prograde_isco, raylist_camera,
+    Tape, TracePipeline, TraceResults, image_camera, oblate_to_cartesian, prograde_isco, raylist_camera,
 )

@@ -85,6 +85,15 @@ class Results(ctypes.Structure):
     _fields_ = [(name, c_void_p) for name in RESULT_FIELDS]
 
 
+class AdjointScene(ctypes.Structure):
+    _fields_ = [("input", SceneInput), ("observer_radius", c_double), ("observer_polar", c_double),
+                ("observer_azimuth", c_double)]
+
+
+class Grads(ctypes.Structure):
+    _fields_ = [("ray_momentum", c_void_p), ("ray_params", c_void_p), ("params", c_void_p)]
+
+
 class LaunchStats(ctypes.Structure):
     _fields_ = [("kernel_launches", c_uint64), ("last_rays", c_uint64), ("last_grid", c_uint32),
                 ("last_block", c_uint32), ("last_persistent", c_uint32), ("sm_count", c_uint32)]
@@ -116,6 +125,12 @@ SIGNATURES = {
     "glc_graph_destroy": (c_int32, [c_void_p]),
     "glc_autotune": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_int32,
                                ctypes.POINTER(Results), c_void_p, c_int32, ctypes.POINTER(Policy)]),
+    "glc_forward_ckpt": (c_int32, [c_void_p, ctypes.POINTER(AdjointScene), ctypes.POINTER(Camera), c_int32,
+                                   ctypes.POINTER(Results), c_void_p, ctypes.POINTER(c_void_p)]),
+    "glc_backward": (c_int32, [c_void_p, c_void_p, ctypes.POINTER(Grads), c_void_p]),
+    "glc_tape_info": (c_int32, [c_void_p, ctypes.POINTER(c_uint64), ctypes.POINTER(c_uint32),
+                                ctypes.POINTER(c_uint64)]),
+    "glc_tape_destroy": (c_int32, [c_void_p]),
     "glc_trace_static_scratch": (c_int32, [c_void_p, c_int32, c_void_p, c_int32, ctypes.POINTER(Policy),
                                            ctypes.POINTER(Results), c_void_p]),
 }

@@ -1,0 +1,481 @@
+// Discrete adjoint over the C ABI: glc_forward_ckpt (trace with per-ray checkpoints every K accepted
+// steps) and glc_backward (segment replay and reverse sweeps). The per-step algebra is in
+// glc_adjoint.cuh; this file holds the kernels, the tape and the host-side scene derivatives.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "glc_adjoint.cuh"
+#include "glc_context.h"
+#include "glc_internal.h"
+#include "glc_kernels.cuh"
+
+using namespace glc;
+
+namespace {
+
+template <int P>
+struct RayWords {
+  static_assert(std::is_trivially_copyable<Ray<P>>::value, "checkpointed rays are copied bytewise");
+  static constexpr int kWords = int((sizeof(Ray<P>) + 15) / 16);
+};
+
+// One attempt with the per-ray shell decision, compiled once so that the forward pass and every
+// backward replay run the identical instruction sequence (bitwise-identical step sequences).
+template <int P>
+__device__ __noinline__ bool adjoint_step(Ray<P>& ray, const LaneScene& ls, const glc_policy& pol,
+                                          RayResult<typename PrecTraits<P>::S>& res) {
+  const bool use64 = P == kMIXED && double(ray.r) < ls.shell_r;
+  return ray.step(ls, pol, res, use64);
+}
+
+// Checkpoint c of ray gi: the ray object as 16-byte words, word-major across rays (coalesced).
+template <int P>
+__device__ __forceinline__ void store_ray(const Ray<P>& ray, uint4* ckpt, uint32_t c, unsigned long long n,
+                                          unsigned long long gi) {
+  constexpr int W = RayWords<P>::kWords;
+  uint4 buf[W];
+  memcpy(buf, &ray, sizeof(Ray<P>));
+#pragma unroll
+  for (int w = 0; w < W; ++w) ckpt[((unsigned long long)c * W + w) * n + gi] = buf[w];
+}
+
+template <int P>
+__device__ __forceinline__ void load_ray(Ray<P>& ray, const uint4* ckpt, uint32_t c, unsigned long long n,
+                                         unsigned long long gi) {
+  constexpr int W = RayWords<P>::kWords;
+  uint4 buf[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) buf[w] = ckpt[((unsigned long long)c * W + w) * n + gi];
+  memcpy(&ray, buf, sizeof(Ray<P>));
+}
+
+// meta per ray: x checkpoints taken, y termination, z accepted steps, w 1 traced / 2 checkpoint
+// capacity exceeded / 0 tile padding. counters: [0] rays over capacity, [1] most accepted steps,
+// [2] replay mismatches, [3] degenerate terminal events.
+template <int P>
+__global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_policy pol, glc_results out,
+                                                              uint32_t K, uint32_t cap, uint4* ckpt, uint4* meta,
+                                                              unsigned int* counters) {
+  using S = typename PrecTraits<P>::S;
+  const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= job.total) return;
+  double st8[8], dir;
+  unsigned long long slot;
+  int scene_idx;
+  bool certified;
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified)) {
+    meta[gi] = make_uint4(0, 0, 0, 0);
+    return;
+  }
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
+  Ray<P> ray;
+  ray.init(ls, pol, st8, dir);
+  RayResult<S> res;
+  uint32_t taken = 0;
+  bool over = false;
+  for (;;) {
+    if (ray.accepted == taken * K) {
+      if (taken < cap) store_ray<P>(ray, ckpt, taken, job.total, gi);
+      else over = true;
+      ++taken;
+    }
+    if (adjoint_step<P>(ray, ls, pol, res)) break;
+  }
+  write_result<P>(out, slot, ray, res, ls);
+  meta[gi] = make_uint4(taken, res.termination, ray.accepted, over ? 2u : 1u);
+  if (over) atomicAdd(counters, 1u);
+  atomicMax(counters + 1, ray.accepted);
+}
+
+// Adjoint of every ray: replay each checkpointed segment (recording the start state and step size
+// of each attempt in scratch, K entries per ray) and sweep it in reverse, last segment first.
+template <int P>
+__global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K,
+                                                               const uint4* ckpt, const uint4* meta, double* scratch,
+                                                               const double* dl, glc_grads g, const double* dconst,
+                                                               double charge, unsigned int* counters) {
+  using S = typename PrecTraits<P>::S;
+  const unsigned long long n = job.total;
+  const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= n) return;
+  const uint4 m = meta[gi];
+  if (m.w == 0u) return;
+  double st8[8], dir;
+  unsigned long long slot;
+  int scene_idx;
+  bool certified;
+  ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified);
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
+  const KN<D9> kd = kn_dual(ls.kn);
+  double wobs[kObs];
+  bool any = false;
+  for (int k = 0; k < kObs; ++k) {
+    wobs[k] = dl[slot * kObs + k];
+    any = any || wobs[k] != 0.0;
+  }
+  double lam[6] = {0, 0, 0, 0, 0, 0}, gacc[3] = {0, 0, 0};
+  const bool differentiable = m.w == 1u && (m.y == GLC_TERM_SURFACE || m.y == GLC_TERM_ESCAPE);
+  bool ok = differentiable && any;
+  bool degenerate = false;
+  double wst[7];
+  step_weights(wst);
+  for (int c = int(m.x) - 1; ok && c >= 0; --c) {
+    Ray<P> ray;
+    load_ray<P>(ray, ckpt, uint32_t(c), n, gi);
+    RayResult<S> res;
+    uint32_t j = 0;
+    bool term = false;
+    for (;;) {
+      if (j >= K) {
+        ok = false;
+        break;
+      }
+      double* rec = scratch + (unsigned long long)j * 7 * n + gi;
+      for (int q = 0; q < 6; ++q) rec[q * n] = double(ray.ys(q));
+      rec[6 * n] = double(ray.h);
+      const uint32_t acc = ray.accepted;
+      if (adjoint_step<P>(ray, ls, pol, res)) {
+        term = true;
+        break;
+      }
+      if (ray.accepted != acc) {
+        ++j;
+        if (ray.accepted == (uint32_t(c) + 1u) * K) break;
+      }
+    }
+    if (!ok) break;
+    const double E = double(ray.E);
+    if (c == int(m.x) - 1) {
+      // the replay must end where the forward pass ended
+      if (!term || res.termination != m.y || ray.accepted != m.z) {
+        ok = false;
+        break;
+      }
+      const double* rec = scratch + (unsigned long long)j * 7 * n + gi;
+      double y0[6];
+      for (int q = 0; q < 6; ++q) y0[q] = rec[q * n];
+      if (!terminal_reverse(ls, y0, E, rec[6 * n], double(res.event_theta), double(ray.dir), m.y, wobs, lam, gacc)) {
+        ok = false;
+        degenerate = true;
+        break;
+      }
+    } else if (term) {
+      ok = false;
+      break;
+    }
+    for (int jj = int(j) - 1; jj >= 0; --jj) {
+      const double* rec = scratch + (unsigned long long)jj * 7 * n + gi;
+      double y0[6], l0[6];
+      for (int q = 0; q < 6; ++q) y0[q] = rec[q * n];
+      dp5_reverse(ls.kn, kd, y0, E, rec[6 * n], wst, lam, l0, gacc);
+      for (int q = 0; q < 6; ++q) lam[q] = l0[q];
+    }
+  }
+  if (!ok) {
+    for (int q = 0; q < 6; ++q) lam[q] = 0.0;
+    gacc[0] = gacc[1] = gacc[2] = 0.0;
+    if (differentiable && any) atomicAdd(counters + (degenerate ? 3 : 2), 1u);
+  }
+  // dL/dp_t = -dL/dE (E = -p_t)
+  const double gpt = -gacc[0];
+  if (g.ray_momentum) {
+    double2* rm = reinterpret_cast<double2*>(g.ray_momentum + 4 * slot);
+    rm[0] = make_double2(gpt, lam[3]);
+    rm[1] = make_double2(lam[4], lam[5]);
+  }
+  double pg[4] = {gacc[1], 2.0 * charge * gacc[2], 0.0, 0.0};
+  const glc_camera& cam = job.cams[0];
+  if (ok && dconst && cam.kind == GLC_CAMERA_PINHOLE) {
+    // the initial state's dependence on (a, Q, inclination, r_obs) through the observer's tetrad
+    const glc_scene& sc = job.scenes[scene_idx];
+    double cv[kSceneConsts];
+    gather_scene_consts(sc, cv);
+    Dual<4> cd[kSceneConsts];
+    for (int i = 0; i < kSceneConsts; ++i) {
+      cd[i] = Dual<4>(cv[i]);
+      for (int k = 0; k < 4; ++k) cd[i].d[k] = dconst[k * kSceneConsts + i];
+    }
+    const unsigned long long pix = slot - cam.result_offset;
+    const double px = double(pix % cam.width) + cam.subpixel_x, py = double(pix / cam.width) + cam.subpixel_y;
+    Dual<4> ds[8];
+    pinhole_state(cd, px, py, double(cam.width), double(cam.height), ds);
+    const double ls8[8] = {0.0, lam[0], lam[1], lam[2], gpt, lam[3], lam[4], lam[5]};
+    for (int i = 0; i < 8; ++i)
+      for (int k = 0; k < 4; ++k) pg[k] += ls8[i] * ds[i].d[k];
+  }
+  if (g.ray_params) {
+    double2* rp = reinterpret_cast<double2*>(g.ray_params + 4 * slot);
+    rp[0] = make_double2(pg[0], pg[1]);
+    rp[1] = make_double2(pg[2], pg[3]);
+  }
+  if (g.params && ok)
+    for (int k = 0; k < 4; ++k)
+      if (pg[k] != 0.0) atomicAdd(g.params + k, pg[k]);
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+void oblate_position(double spin, int chart, double r, double polar, double azimuth, double out[4]) {
+  // KerrNewmanSpacetime::oblate_to_cartesian (crates/gravlume-domain/src/spacetime.rs:245-254)
+  const double st = std::sin(polar), ct = std::cos(polar), sp = std::sin(azimuth), cp = std::cos(azimuth);
+  const double cs = (chart == GLC_CHART_INGOING ? 1.0 : -1.0) * spin;
+  out[0] = 0.0;
+  out[1] = (cs * -sp + r * cp) * st;
+  out[2] = (cs * cp + r * sp) * st;
+  out[3] = r * ct;
+}
+
+// p = (a, Q, inclination, r_obs)
+glc_status pack_adjoint_scene(const glc_adjoint_scene& as, const double p[4], glc_scene& out) {
+  glc_scene_input in = as.input;
+  in.spin = p[0];
+  in.charge = p[1];
+  oblate_position(p[0], in.chart, p[3], p[2], as.observer_azimuth, in.observer_txyz);
+  return pack_scene(in, out);
+}
+
+}  // namespace
+
+struct glc_tape {
+  glc_ctx* ctx = nullptr;
+  glc_policy pol{};
+  glc_camera cam{};
+  uint32_t K = 0, cap = 0, words = 0;
+  unsigned long long n = 0;
+  double charge = 0.0;
+  unsigned char* d_job = nullptr;
+  size_t off_cams = 0, off_begin = 0, off_cert = 0;
+  uint4* d_ckpt = nullptr;
+  size_t ckpt_bytes = 0;
+  uint4* d_meta = nullptr;
+  double* d_dconst = nullptr;
+  double* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  unsigned int* d_counters = nullptr;
+  bool pinhole = false;
+
+  JobView job() const {
+    JobView v;
+    v.scenes = reinterpret_cast<const glc_scene*>(d_job);
+    v.cams = reinterpret_cast<const glc_camera*>(d_job + off_cams);
+    v.begin = reinterpret_cast<const unsigned long long*>(d_job + off_begin);
+    v.cert_begin = reinterpret_cast<const unsigned long long*>(d_job + off_cert);
+    v.cert = nullptr;
+    v.n_cams = 1;
+    v.total = n;
+    return v;
+  }
+};
+
+namespace {
+
+void free_tape(glc_tape* t) {
+  if (!t) return;
+  if (t->d_job) cudaFree(t->d_job);
+  if (t->d_ckpt) cudaFree(t->d_ckpt);
+  if (t->d_meta) cudaFree(t->d_meta);
+  if (t->d_dconst) cudaFree(t->d_dconst);
+  if (t->d_scratch) cudaFree(t->d_scratch);
+  if (t->d_counters) cudaFree(t->d_counters);
+  delete t;
+}
+
+glc_status cuda_status(cudaError_t e) {
+  return e == cudaSuccess ? GLC_OK : set_error(GLC_ERR_CUDA, cudaGetErrorString(e));
+}
+
+template <int P>
+glc_status run_forward(glc_tape* t, const glc_results& out, cudaStream_t st) {
+  const unsigned grid = unsigned((t->n + 127) / 128);
+  glc_status s = cuda_status(cudaMemsetAsync(t->d_counters, 0, 4 * sizeof(unsigned int), st));
+  if (s != GLC_OK) return s;
+  adjoint_forward_kernel<P><<<grid, 128, 0, st>>>(t->job(), t->pol, out, t->K, t->cap, t->d_ckpt, t->d_meta,
+                                                   t->d_counters);
+  s = cuda_status(cudaGetLastError());
+  if (s == GLC_OK) t->ctx->stats.kernel_launches += 1;
+  return s;
+}
+
+glc_status forward(glc_tape* t, const glc_results& out, cudaStream_t st) {
+  return t->pol.precision == GLC_MIXED ? run_forward<kMIXED>(t, out, st) : run_forward<kFP64>(t, out, st);
+}
+
+glc_status size_checkpoints(glc_tape* t, uint32_t cap) {
+  if (t->d_ckpt) cudaFree(t->d_ckpt);
+  t->d_ckpt = nullptr;
+  t->cap = cap;
+  t->ckpt_bytes = size_t(cap) * t->words * 16 * t->n;
+  return cuda_status(cudaMalloc(&t->d_ckpt, t->ckpt_bytes));
+}
+
+struct DeviceScope {
+  int prev = -1, want = 0;
+  explicit DeviceScope(int dev) : want(dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    if (prev >= 0 && prev != want) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc_camera* camera, int32_t K,
+                            const glc_results* out, void* stream, glc_tape** tape) {
+  if (!ctx || !as || !camera || !out || !tape) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  *tape = nullptr;
+  if (K < 1) return set_error(GLC_ERR_INVALID_ARGUMENT, "checkpoint interval K must be at least 1");
+  const glc_policy pol = ctx->policy;
+  if (pol.precision != GLC_MIXED && pol.precision != GLC_FP64)
+    return set_error(GLC_ERR_UNSUPPORTED, "the adjoint runs in MIXED or FP64 precision");
+  if (camera->kind != GLC_CAMERA_PINHOLE && camera->kind != GLC_CAMERA_RAYLIST)
+    return set_error(GLC_ERR_UNSUPPORTED, "the adjoint takes a pinhole or ray-list camera");
+  if (camera->scene_index != 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera must use scene 0");
+  if (!(as->observer_radius > 0.0) || !std::isfinite(as->observer_polar) || !std::isfinite(as->observer_azimuth))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "observer oblate coordinates must be finite, radius positive");
+  const double p0[4] = {as->input.spin, as->input.charge, as->observer_polar, as->observer_radius};
+  glc_scene scene;
+  glc_status s = pack_adjoint_scene(*as, p0, scene);
+  if (s != GLC_OK) return s;
+  unsigned long long n = 0;
+  if (camera->kind == GLC_CAMERA_PINHOLE) {
+    if (camera->width != scene.width || camera->height != scene.height)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "pinhole camera size must match the scene's view");
+    if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
+    const unsigned long long tx = (camera->width + pol.tile_w - 1) / pol.tile_w;
+    const unsigned long long ty = (camera->height + pol.tile_h - 1) / pol.tile_h;
+    n = tx * ty * pol.tile_w * pol.tile_h;
+  } else {
+    if (!camera->ray_states || (reinterpret_cast<uintptr_t>(camera->ray_states) & 15u) != 0)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "ray states must be a 16-byte aligned device array");
+    if (!(camera->affine_direction == 1.0 || camera->affine_direction == -1.0))
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "affine direction must be +1 or -1");
+    n = camera->n_rays;
+  }
+  if (n == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "no rays");
+
+  // scene-constant derivatives with respect to (a, Q, inclination, r_obs): central differences of
+  // the host scene pack (the tetrad construction is not differentiated on the device)
+  double dconst[4 * kSceneConsts] = {};
+  const bool pinhole = camera->kind == GLC_CAMERA_PINHOLE;
+  if (pinhole) {
+    const double step[4] = {1e-6, 1e-6, 1e-6, 1e-6 * as->observer_radius};
+    for (int k = 0; k < 4; ++k) {
+      double pp[4], pm[4];
+      std::memcpy(pp, p0, sizeof(pp));
+      std::memcpy(pm, p0, sizeof(pm));
+      pp[k] += step[k];
+      pm[k] -= step[k];
+      glc_scene sp, sm;
+      s = pack_adjoint_scene(*as, pp, sp);
+      if (s == GLC_OK) s = pack_adjoint_scene(*as, pm, sm);
+      if (s != GLC_OK) return set_error(s, "scene derivative: a perturbed scene is invalid");
+      double cp[kSceneConsts], cm[kSceneConsts];
+      gather_scene_consts(sp, cp);
+      gather_scene_consts(sm, cm);
+      for (int i = 0; i < kSceneConsts; ++i) dconst[k * kSceneConsts + i] = (cp[i] - cm[i]) / (2.0 * step[k]);
+    }
+  }
+
+  DeviceScope scope(ctx->device);
+  glc_tape* t = new glc_tape();
+  t->ctx = ctx;
+  t->pol = pol;
+  t->cam = *camera;
+  t->K = uint32_t(K);
+  t->n = n;
+  t->charge = scene.charge;
+  t->pinhole = pinhole;
+  t->words = uint32_t(pol.precision == GLC_MIXED ? RayWords<kMIXED>::kWords : RayWords<kFP64>::kWords);
+  t->off_cams = align256(sizeof(glc_scene));
+  t->off_begin = t->off_cams + align256(sizeof(glc_camera));
+  t->off_cert = t->off_begin + 256;
+  const size_t job_bytes = t->off_cert + 256;
+  auto fail = [&](glc_status st) {
+    free_tape(t);
+    return st;
+  };
+  alignas(16) static thread_local unsigned char host_job[4096];
+  std::memset(host_job, 0, sizeof(host_job));
+  std::memcpy(host_job, &scene, sizeof(glc_scene));
+  std::memcpy(host_job + t->off_cams, camera, sizeof(glc_camera));
+  const unsigned long long begin[2] = {0, n}, cert_begin[2] = {0, 0};
+  std::memcpy(host_job + t->off_begin, begin, sizeof(begin));
+  std::memcpy(host_job + t->off_cert, cert_begin, sizeof(cert_begin));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMalloc(&t->d_job, job_bytes) != cudaSuccess || cudaMalloc(&t->d_meta, n * sizeof(uint4)) != cudaSuccess ||
+      cudaMalloc(&t->d_dconst, sizeof(dconst)) != cudaSuccess ||
+      cudaMalloc(&t->d_counters, 4 * sizeof(unsigned int)) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "tape allocation failed"));
+  // pageable sources: both copies have consumed their bytes when they return
+  if (cudaMemcpyAsync(t->d_job, host_job, job_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(t->d_dconst, dconst, sizeof(dconst), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "tape upload failed"));
+  // checkpoint slots for 512 accepted steps; when a ray needs more, the pass runs again with the
+  // capacity its longest ray needs
+  s = size_checkpoints(t, uint32_t(512 / t->K + 2));
+  if (s == GLC_OK) s = forward(t, *out, st);
+  if (s != GLC_OK) return fail(s);
+  unsigned int counters[4];
+  if (cudaMemcpyAsync(counters, t->d_counters, sizeof(counters), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return fail(set_error(GLC_ERR_CUDA, "forward pass failed"));
+  if (counters[0] > 0) {
+    s = size_checkpoints(t, counters[1] / t->K + 2);
+    if (s == GLC_OK) s = forward(t, *out, st);
+    if (s != GLC_OK) return fail(s);
+  }
+  *tape = t;
+  return GLC_OK;
+}
+
+glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, void* stream) {
+  if (!t || !dl || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceScope scope(t->ctx->device);
+  const size_t need = size_t(t->K) * 7 * sizeof(double) * t->n;
+  if (need > t->scratch_bytes) {
+    if (t->d_scratch) cudaFree(t->d_scratch);
+    t->d_scratch = nullptr;
+    t->scratch_bytes = 0;
+    if (cudaMalloc(&t->d_scratch, need) != cudaSuccess)
+      return set_error(GLC_ERR_CUDA, "adjoint scratch allocation failed");
+    t->scratch_bytes = need;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned grid = unsigned((t->n + 127) / 128);
+  const double* dconst = t->pinhole ? t->d_dconst : nullptr;
+  if (t->pol.precision == GLC_MIXED)
+    adjoint_backward_kernel<kMIXED><<<grid, 128, 0, st>>>(t->job(), t->pol, t->K, t->d_ckpt, t->d_meta, t->d_scratch,
+                                                          dl, *out, dconst, t->charge, t->d_counters);
+  else
+    adjoint_backward_kernel<kFP64><<<grid, 128, 0, st>>>(t->job(), t->pol, t->K, t->d_ckpt, t->d_meta, t->d_scratch,
+                                                         dl, *out, dconst, t->charge, t->d_counters);
+  const glc_status s = cuda_status(cudaGetLastError());
+  if (s == GLC_OK) t->ctx->stats.kernel_launches += 1;
+  return s;
+}
+
+glc_status glc_tape_info(const glc_tape* t, uint64_t* rays, uint32_t* slots, uint64_t* bytes) {
+  if (!t) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (rays) *rays = t->n;
+  if (slots) *slots = t->cap;
+  if (bytes) *bytes = t->ckpt_bytes + t->scratch_bytes + t->n * sizeof(uint4);
+  return GLC_OK;
+}
+
+glc_status glc_tape_destroy(glc_tape* t) {
+  if (!t) return GLC_OK;
+  DeviceScope scope(t->ctx->device);
+  cudaDeviceSynchronize();
+  free_tape(t);
+  return GLC_OK;
+}
+
+}  // extern "C"

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "glc_context.h"
 #include "glc_internal.h"
 #include "glc_certificate.cuh"
 
@@ -130,24 +131,6 @@ JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
 }
 
 }  // namespace
-
-struct glc_ctx {
-  int device = 0;
-  int sm_count = 0;
-  glc_policy policy{};
-  unsigned char* d_job = nullptr;
-  size_t d_job_bytes = 0;
-  unsigned char* h_stage = nullptr;
-  size_t h_stage_bytes = 0;
-  cudaEvent_t stage_free = nullptr;  // recorded after the last staging copy
-  bool stage_pending = false;
-  unsigned long long* d_queue = nullptr;
-  uint32_t* d_cert = nullptr;          // per-tile capture certificates (grow-only)
-  size_t d_cert_words = 0;
-  unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
-  size_t d_host_ws_bytes = 0;
-  glc_launch_stats stats{};
-};
 
 struct glc_graph {
   glc_ctx* ctx = nullptr;

@@ -153,6 +153,7 @@ template <class S>
 struct RayResult {
   uint32_t termination, failure, candidates, flags;
   S event_residual;
+  S event_theta;  // fraction of the terminal step at the localized event (read by the adjoint)
   S escape_theta, escape_phi;
   S surface_r, surface_phi, g;
 };
@@ -247,9 +248,10 @@ GLC_HD bool localize(const T y0[6], T h, const DensePoly<T>& K, T tol, T sv, T e
 
 // Keplerian prograde circular emitter observable (surface.rs:75-146, M = 1). Returns false when
 // the orbit is unavailable or not timelike.
+// frequency_ratio: g of the emitter at radius r for a photon with energy E and state y (a, Q^2 and
+// a^2 as T so that the adjoint can differentiate through them).
 template <class T>
-GLC_HD bool surface_observable(const LaneScene& sc, const T y[6], T E, T r, T& g, T& phi_s) {
-  const T a = T(sc.kn.a), q2 = T(sc.kn.q2), a2 = T(sc.kn.a2);
+GLC_HD bool frequency_ratio(T a, T q2, T a2, double frequency, const T y[6], T E, T r, T& g) {
   const T crs = r - q2;
   if (!(crs >= T(0))) return false;
   const T cr = g_sqrt(crs);
@@ -272,9 +274,15 @@ GLC_HD bool surface_observable(const LaneScene& sc, const T y[6], T E, T r, T& g
   const T lz = y[0] * y[4] - y[1] * y[3];
   const T ef = ut * (E - omega * lz);
   if (!(ef > T(0))) return false;
-  g = T(sc.frequency) / ef;
-  phi_s = wrapped_angle(g_atan2(y[1], y[0]), g_atan2(T(sc.kn.sa), r));
+  g = T(frequency) / ef;
   return g_finite(g) && g > T(0);
+}
+
+template <class T>
+GLC_HD bool surface_observable(const LaneScene& sc, const T y[6], T E, T r, T& g, T& phi_s) {
+  if (!frequency_ratio(T(sc.kn.a), T(sc.kn.q2), T(sc.kn.a2), sc.frequency, y, E, r, g)) return false;
+  phi_s = wrapped_angle(g_atan2(y[1], y[0]), g_atan2(T(sc.kn.sa), r));
+  return true;
 }
 
 // Renormalize the spatial momentum so that g^{mu nu} p_mu p_nu = 0 (scaling p_i by lambda closest
@@ -801,6 +809,7 @@ struct Ray {
     else if (kind == kEvSurface) term = GLC_TERM_SURFACE;
     else if (kind == kEvEscape) term = GLC_TERM_ESCAPE;
     finish_event(sc, pol, res, term, cand, residuals[first], ycommit);
+    res.event_theta = term_theta;
     return true;
   }
 
@@ -810,6 +819,7 @@ struct Ray {
     res.candidates = 0;
     res.flags = flags;
     res.event_residual = S(NAN);
+    res.event_theta = S(NAN);
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
   }

@@ -209,6 +209,50 @@ class TraceResults:
         return out
 
 
+class Tape:
+    """Checkpoints of a forward trace (glc_forward_ckpt); backward() runs the discrete adjoint."""
+
+    def __init__(self, handle, pipeline, slots: int, keepalive):
+        self.handle = handle
+        self.pipeline = pipeline
+        self.slots = slots
+        self._keep = keepalive
+
+    def info(self) -> dict:
+        rays, cap, nbytes = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint64()
+        N.check(N.lib().glc_tape_info(self.handle, ctypes.byref(rays), ctypes.byref(cap), ctypes.byref(nbytes)),
+                "glc_tape_info")
+        return {"rays": rays.value, "checkpoint_slots": cap.value, "bytes": nbytes.value}
+
+    def backward(self, dl_dobs, stream=None, per_ray_params: bool = True) -> dict:
+        """dl_dobs: (slots, 4) float64 dL/d(source radius, g, escape theta, escape phi). Returns device
+        tensors ray_momentum (slots, 4) dL/d(p_t, p_x, p_y, p_z), ray_params (slots, 4) and params (4,)
+        dL/d(a, Q, inclination, r_obs)."""
+        torch = _torch()
+        dev = torch.device("cuda", self.pipeline.device)
+        dl = torch.as_tensor(dl_dobs).to(device=dev, dtype=torch.float64).contiguous()
+        assert tuple(dl.shape) == (self.slots, 4)
+        mom = torch.zeros((self.slots, 4), dtype=torch.float64, device=dev)
+        rp = torch.zeros((self.slots, 4), dtype=torch.float64, device=dev) if per_ray_params else None
+        params = torch.zeros(4, dtype=torch.float64, device=dev)
+        g = N.Grads(mom.data_ptr(), rp.data_ptr() if rp is not None else None, params.data_ptr())
+        N.check(N.lib().glc_backward(self.handle, ctypes.c_void_p(dl.data_ptr()), ctypes.byref(g),
+                                     self.pipeline._stream(stream)), "glc_backward")
+        self._last = (dl, mom, rp, params)
+        return {"ray_momentum": mom, "ray_params": rp, "params": params}
+
+    def close(self):
+        if self.handle:
+            N.lib().glc_tape_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Graph:
     def __init__(self, handle: int, keepalive):
         self.handle = handle
@@ -322,6 +366,32 @@ class TracePipeline:
         N.check(N.lib().glc_trace(self._h, sa, len(scenes), ca, len(cameras), ctypes.byref(rs),
                                   self._stream(stream)), "glc_trace")
         return results
+
+    def forward_ckpt(self, observation: Observation, radius: float, polar: float, azimuth: float = 0.0,
+                     K: int = 64, states=None, direction: float = -1.0, stream=None):
+        """Forward trace with checkpoints every K accepted steps (glc_forward_ckpt). The observer sits
+        at oblate (radius, polar, azimuth); the camera is the observation's pinhole view, or the ray
+        list `states` (n, 8). Returns (TraceResults, Tape)."""
+        torch = _torch()
+        a = N.AdjointScene()
+        a.input = observation.scene_input()
+        a.observer_radius, a.observer_polar, a.observer_azimuth = radius, polar, azimuth
+        keep = []
+        if states is None:
+            cam = image_camera(0, observation.width, observation.height)
+            slots = observation.width * observation.height
+        else:
+            st = torch.as_tensor(np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)).to(
+                torch.device("cuda", self.device))
+            keep.append(st)
+            cam = raylist_camera(0, st.data_ptr(), st.shape[0], direction)
+            slots = st.shape[0]
+        res = TraceResults(slots, torch.device("cuda", self.device))
+        rs = res.struct()
+        h = ctypes.c_void_p()
+        N.check(N.lib().glc_forward_ckpt(self._h, ctypes.byref(a), ctypes.byref(cam), int(K), ctypes.byref(rs),
+                                         self._stream(stream), ctypes.byref(h)), "glc_forward_ckpt")
+        return res, Tape(h, self, slots, keep)
 
     def trace_image(self, observation: Observation, subpixel=(0.5, 0.5), stream=None, **kw) -> TraceResults:
         sc = observation.packed

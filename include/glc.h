@@ -259,6 +259,42 @@ glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
                         int32_t n_cameras, const glc_results* out, void* stream, int32_t repeats,
                         glc_policy* policy);
 
+/* ---- discrete adjoint (forward with checkpoints, backward) --------------------------------- */
+/* Gradients of per-ray observables (source radius, g, escape theta, escape phi) with respect to
+ * spin a, charge Q, observer inclination, observer radius (the observer sits at fixed oblate
+ * coordinates) and each ray's initial covariant momentum. The reference has no adjoint; these are
+ * the forward/backward pair over the trace boundary of glc_trace (trace.rs:701-710 for images,
+ * geodesic.rs:53-62 for explicit ray lists). Precision MIXED or FP64 (the context's policy). */
+typedef struct glc_tape glc_tape;
+
+typedef struct glc_adjoint_scene {
+  glc_scene_input input;          /* observer_txyz is replaced by the oblate position below */
+  double observer_radius;         /* oblate (Boyer-Lindquist) radius of the observer */
+  double observer_polar;          /* inclination, radians */
+  double observer_azimuth;
+} glc_adjoint_scene;
+
+typedef struct glc_grads {
+  double* ray_momentum;           /* device, slots x 4: dL/d(p_t, p_x, p_y, p_z) at the initial state */
+  double* ray_params;             /* device, slots x 4 or NULL: each ray's share of dL/d(a, Q, incl, r_obs) */
+  double* params;                 /* device, 4 or NULL: dL/d(a, Q, inclination, r_obs), ADDED to (caller zeroes) */
+} glc_grads;
+
+/* Forward trace of one camera (PINHOLE of the scene's view, or RAYLIST) that also checkpoints each
+ * ray's stepper state every K accepted steps into the tape (device memory owned by the tape).
+ * Results as glc_trace. The MIXED shell decision is taken per ray (glc_trace takes it per warp), so
+ * the backward pass can replay every segment exactly. Synchronizes the stream once (to size the
+ * checkpoints). */
+glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* scene, const glc_camera* camera, int32_t K,
+                            const glc_results* out, void* stream, glc_tape** tape);
+/* Backward pass: dL_dobs is device, slots x 4 (dL/d source radius, g, escape theta, escape phi;
+ * rays that end elsewhere get zero gradients). Replays each checkpointed segment and sweeps it in
+ * reverse (binary64). Asynchronous on the stream. */
+glc_status glc_backward(glc_tape* tape, const double* dL_dobs, const glc_grads* out, void* stream);
+/* Checkpoint sizing: rays traced, checkpoint slots per ray, device bytes held by the tape. */
+glc_status glc_tape_info(const glc_tape* tape, uint64_t* rays, uint32_t* slots_per_ray, uint64_t* bytes);
+glc_status glc_tape_destroy(glc_tape* tape);
+
 /* ---- trace without device allocation ------------------------------------------------------ */
 /* No counterpart in the reference: its wgpu trace pass always allocates its own target and
  * scratch. For callers that may not allocate device memory (a host whose frame allocator owns the

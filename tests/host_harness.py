@@ -31,6 +31,10 @@ def lib():
         L = ctypes.CDLL(str(OUT))
         L.host_trace_states.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                         ctypes.c_double, ctypes.c_void_p]
+        L.host_adjoint_states.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+        L.host_trace_perturbed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
         assert L.host_trace_fields() == len(FIELDS)
         _lib = L
     return _lib
@@ -45,3 +49,25 @@ def trace_states(scene, policy, states, direction):
     d = {k: out[:, i] for i, k in enumerate(FIELDS)}
     d["termination"] = d["termination"].astype(int)
     return d
+
+
+def adjoint_states(scene, policy, states, direction, dl_dobs):
+    """Per ray: dL/d(x, y, z, p_x, p_y, p_z) at the initial state, dL/dE, dL/da, dL/dQ^2,
+    termination, ok flag, accepted steps (the device adjoint's sweeps, compiled for the host)."""
+    st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+    w = np.ascontiguousarray(dl_dobs, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((st.shape[0], 12))
+    rc = lib().host_adjoint_states(ctypes.byref(scene), ctypes.byref(policy), st.shape[0], st.ctypes.data,
+                                   direction, w.ctypes.data, out.ctypes.data)
+    assert rc == 0
+    return out
+
+
+def trace_perturbed(scene, policy, states, direction, da=0.0, dq2=0.0):
+    """Termination, source radius, g, escape theta, escape phi under spin/charge^2 shifted in the dynamics."""
+    st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+    out = np.zeros((st.shape[0], 5))
+    rc = lib().host_trace_perturbed(ctypes.byref(scene), ctypes.byref(policy), st.shape[0], st.ctypes.data,
+                                    direction, da, dq2, out.ctypes.data)
+    assert rc == 0
+    return out

@@ -5,7 +5,9 @@
 // taken per ray here (the kernels take it per warp).
 #include <cstdint>
 
-#include "../../gravlume_b200/csrc/glc_tracer.cuh"
+#include <vector>
+
+#include "../../gravlume_b200/csrc/glc_adjoint.cuh"
 
 using namespace glc;
 
@@ -59,6 +61,102 @@ extern "C" int host_trace_states(const glc_scene* sc, const glc_policy* pol, int
     case 0: run<kFP32>(*sc, *pol, n, states, dir, out, 29); return 0;
     case 1: run<kMIXED>(*sc, *pol, n, states, dir, out, 29); return 0;
     case 2: run<kFP64>(*sc, *pol, n, states, dir, out, 29); return 0;
+  }
+  return -1;
+}
+
+// Discrete adjoint of whole traces, every accepted step recorded (no checkpoints): for each ray,
+// dL/d(initial x, y, z, p_x, p_y, p_z), dL/dE, dL/da, dL/dQ^2 for the observable weights wobs
+// (source radius, g, escape theta, escape phi). out: 9 gradients, termination, ok, accepted steps.
+namespace {
+template <int P>
+void adjoint(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st, double dir, const double* wobs,
+             double* out) {
+  const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor);
+  const KN<D9> kd = kn_dual(ls.kn);
+  for (int64_t i = 0; i < n; ++i) {
+    Ray<P> ray;
+    ray.init(ls, pol, st + 8 * i, dir);
+    RayResult<typename PrecTraits<P>::S> res;
+    std::vector<double> tape;  // per accepted step: y0[6], h
+    double y0[6], h0 = 0.0;
+    for (;;) {
+      for (int c = 0; c < 6; ++c) y0[c] = double(ray.ys(c));
+      h0 = double(ray.h);
+      const uint32_t acc = ray.accepted;
+      const bool use64 = P == kMIXED && double(ray.r) < ls.shell_r;
+      if (ray.step(ls, pol, res, use64)) break;
+      if (ray.accepted != acc) {
+        tape.insert(tape.end(), y0, y0 + 6);
+        tape.push_back(h0);
+      }
+    }
+    double* o = out + 12 * i;
+    for (int c = 0; c < 12; ++c) o[c] = 0.0;
+    o[9] = res.termination;
+    o[11] = double(tape.size() / 7);
+    double lam[6], g[3] = {0, 0, 0};
+    const double E = double(ray.E);
+    if (!terminal_reverse(ls, y0, E, h0, double(res.event_theta), dir, res.termination, wobs + kObs * i, lam, g))
+      continue;
+    double w[7];
+    step_weights(w);
+    for (size_t m = tape.size() / 7; m-- > 0;) {
+      const double* rec = tape.data() + 7 * m;
+      double l0[6];
+      dp5_reverse(ls.kn, kd, rec, E, rec[6], w, lam, l0, g);
+      for (int c = 0; c < 6; ++c) lam[c] = l0[c];
+    }
+    for (int c = 0; c < 6; ++c) o[c] = lam[c];
+    o[6] = g[0];
+    o[7] = g[1];
+    o[8] = g[2];
+    o[10] = 1.0;
+  }
+}
+
+// Observables of traces under a scene whose spin and squared charge are shifted by (da, dq2) in the
+// dynamics only (the initial states are given): termination, source radius, g, escape theta, phi.
+template <int P>
+void perturbed(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st, double dir, double da,
+               double dq2, double* out) {
+  LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor);
+  ls.kn.a += da;
+  ls.kn.a2 = ls.kn.a * ls.kn.a;
+  ls.kn.sa = ls.kn.s * ls.kn.a;
+  ls.kn.q2 += dq2;
+  for (int64_t i = 0; i < n; ++i) {
+    Ray<P> ray;
+    ray.init(ls, pol, st + 8 * i, dir);
+    RayResult<typename PrecTraits<P>::S> res;
+    for (;;) {
+      const bool use64 = P == kMIXED && double(ray.r) < ls.shell_r;
+      if (ray.step(ls, pol, res, use64)) break;
+    }
+    double* o = out + 5 * i;
+    o[0] = res.termination;
+    o[1] = double(res.surface_r);
+    o[2] = double(res.g);
+    o[3] = double(res.escape_theta);
+    o[4] = double(res.escape_phi);
+  }
+}
+}  // namespace
+
+extern "C" int host_adjoint_states(const glc_scene* sc, const glc_policy* pol, int64_t n, const double* states,
+                                   double dir, const double* wobs, double* out) {
+  switch (pol->precision) {
+    case 1: adjoint<kMIXED>(*sc, *pol, n, states, dir, wobs, out); return 0;
+    case 2: adjoint<kFP64>(*sc, *pol, n, states, dir, wobs, out); return 0;
+  }
+  return -1;
+}
+
+extern "C" int host_trace_perturbed(const glc_scene* sc, const glc_policy* pol, int64_t n, const double* states,
+                                    double dir, double da, double dq2, double* out) {
+  switch (pol->precision) {
+    case 1: perturbed<kMIXED>(*sc, *pol, n, states, dir, da, dq2, out); return 0;
+    case 2: perturbed<kFP64>(*sc, *pol, n, states, dir, da, dq2, out); return 0;
   }
   return -1;
 }
