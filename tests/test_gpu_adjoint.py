@@ -1,0 +1,147 @@
+"""The discrete adjoint on the GPU (glc_forward_ckpt / glc_backward) through the C ABI.
+
+1. Ray lists: the device gradients with respect to the initial momentum, spin and charge equal the
+   host-compiled adjoint of the same traces (itself checked against finite differences in
+   tests/test_adjoint_host.py) to 1e-8 relative, and do not depend on the checkpoint interval K.
+2. Pinhole frames, binary64 and mixed forward passes: the gradients with respect to (a, Q,
+   inclination, r_obs), which also flow through the observer tetrad, agree with central differences
+   (h = 1e-6) of the binary64 oracle at rtol 1e-12 to 1e-4 relative (the adjoint's precision
+   target), both summed over the rays whose termination class is unchanged by the perturbations and
+   per ray at the 95th percentile.
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import gravlume_b200 as G
+import host_harness as H
+import oracle as O
+from gpu_common import config1_observation, oracle_for
+
+pytestmark = pytest.mark.gpu
+
+SURF, ESC = G.Termination.EQUATORIAL_SURFACE, G.Termination.ESCAPE
+
+
+@pytest.fixture(scope="module")
+def pipe():
+    p = G.TracePipeline(0)
+    yield p
+    p.close()
+
+
+def tight(precision=G.Precision.FP64, rtol=1e-12):
+    return G.ReferencePolicy.frame(precision, position_rtol=rtol, momentum_rtol=rtol, position_atol=rtol * 1e-2,
+                                   momentum_atol=rtol * 1e-2)
+
+
+def weights(term):
+    w = np.zeros((term.size, 4))
+    w[term == SURF, 0], w[term == SURF, 1] = 1.0, 10.0
+    w[term == ESC, 2], w[term == ESC, 3] = 1.0, 1.0
+    return w
+
+
+def test_ray_list_adjoint_matches_the_host_adjoint_for_every_checkpoint_interval(pipe):
+    obs = config1_observation(width=64, height=64)
+    osc, ev, sc = oracle_for(obs)
+    rng = np.random.default_rng(21)
+    states, _, _, status = O.initial_rays(osc, rng.integers(4, 60, 96), rng.integers(4, 60, 96))
+    assert (status == 0).all()
+    states = np.asarray(states)
+    pol = tight()
+    base = H.trace_perturbed(sc, pol, states, -1.0)
+    w = weights(base[:, 0].astype(int))
+    host = H.adjoint_states(sc, pol, states, -1.0, w)
+    want_mom = np.stack([-host[:, 6], host[:, 3], host[:, 4], host[:, 5]], axis=1)
+    want_par = np.stack([host[:, 7], 2 * 0.3 * host[:, 8]], axis=1)
+    pipe.set_policy(pol)
+    got = {}
+    for K in (1, 4, 64):
+        res, tape = pipe.forward_ckpt(obs, 50.0, math.radians(75.0), K=K, states=states)
+        g = tape.backward(w)
+        torch.cuda.synchronize()
+        d = res.numpy()
+        np.testing.assert_array_equal(d["termination"], base[:, 0].astype(int))
+        got[K] = (g["ray_momentum"].cpu().numpy(), g["ray_params"].cpu().numpy())
+        tape.close()
+    for K, (mom, par) in got.items():
+        scale = np.maximum(np.abs(want_mom).max(axis=1), 1e-300)[:, None]
+        err = np.abs(mom - want_mom) / scale
+        print("K", K, "momentum max rel", float(err.max()))
+        assert err.max() <= 1e-8, K
+        perr = np.abs(par[:, :2] - want_par) / np.maximum(np.abs(want_par).max(axis=1), 1e-300)[:, None]
+        assert perr.max() <= 1e-8, K
+    np.testing.assert_array_equal(got[1][0], got[64][0])
+
+
+def observation(a, q, incl, r_obs, isco, n):
+    return G.Observation.from_oblate(r_obs, incl, 0.0, spin=a, charge=q, chart=G.KerrSchildChart.OUTGOING,
+                                     width=n, height=n, vertical_fov=math.radians(30.0), escape_radius=1000.0,
+                                     surface=G.EquatorialSurface(isco, 20.0), horizon_offset=1e-3)
+
+
+def oracle_obs(obs_, px, py):
+    osc, ev, _ = oracle_for(obs_)
+    ref, status = O.trace_pixels(osc, O.custom_policy(1e-12, 1e-14), ev, px, py, threads=O.hardware_threads())
+    assert (status == 0).all()
+    F = O.F
+    out = np.stack([ref[:, F["source_radius"]], ref[:, F["frequency_ratio"]], np.zeros(len(px)),
+                    np.zeros(len(px))], axis=1)
+    esc = ref[:, F["termination"]].astype(int) == ESC
+    d = np.stack([ref[:, F["escape_dx"]], ref[:, F["escape_dy"]], ref[:, F["escape_dz"]]], axis=1)
+    out[esc, 2] = np.arccos(np.clip(d[esc, 2], -1, 1))
+    out[esc, 3] = np.arctan2(d[esc, 1], d[esc, 0])
+    return ref[:, F["termination"]].astype(int), out
+
+
+@pytest.mark.parametrize("precision", [G.Precision.FP64, G.Precision.MIXED])
+def test_scene_parameter_gradients_match_oracle_central_differences(pipe, precision):
+    a, q, incl, r_obs, n = 0.9, 0.3, math.radians(60.0), 50.0, 24
+    isco = G.prograde_isco(a, q)
+    obs = observation(a, q, incl, r_obs, isco, n)
+    pipe.set_policy(tight(G.Precision.FP64, 1e-10) if precision == G.Precision.FP64 else
+                    G.ReferencePolicy.frame(G.Precision.MIXED))
+    res, tape = pipe.forward_ckpt(obs, r_obs, incl, K=16)
+    d = res.numpy()
+    term = d["termination"]
+    w = weights(term)
+    g = tape.backward(w)
+    torch.cuda.synchronize()
+    per_ray = g["ray_params"].cpu().numpy()
+    total = g["params"].cpu().numpy()
+    np.testing.assert_allclose(per_ray.sum(axis=0), total, rtol=1e-12, atol=1e-12)
+    tape.close()
+    idx = np.arange(n * n)
+    px, py = idx % n, idx // n
+    base_t, base_o = oracle_obs(obs, px, py)
+    steps = [1e-6, 1e-6, 1e-6, 1e-6 * r_obs]
+    stable = (base_t == term) & np.isin(term, [SURF, ESC])
+    fd = np.zeros((n * n, 4))
+    params = [a, q, incl, r_obs]
+    for k in range(4):
+        outs = []
+        for sgn in (1, -1):
+            p = list(params)
+            p[k] += sgn * steps[k]
+            t_, o_ = oracle_obs(observation(p[0], p[1], p[2], p[3], isco, n), px, py)
+            stable &= t_ == base_t
+            outs.append(o_)
+        dphi = (outs[0][:, 3] - outs[1][:, 3] + math.pi) % (2 * math.pi) - math.pi
+        diff = outs[0] - outs[1]
+        diff[:, 3] = dphi
+        fd[:, k] = (w * diff).sum(axis=1) / (2 * steps[k])
+    # rays whose escape direction sits on the azimuth branch cut or whose observables jump are unstable
+    assert stable.sum() >= 0.8 * np.isin(term, [SURF, ESC]).sum()
+    adj_sum = per_ray[stable].sum(axis=0)
+    fd_sum = fd[stable].sum(axis=0)
+    rel = np.abs(adj_sum - fd_sum) / np.maximum(np.abs(fd_sum), 1e-12)
+    scale = np.maximum(np.abs(fd[stable]).max(axis=1), 1e-12)
+    per_rel = np.abs(per_ray[stable] - fd[stable]).max(axis=1) / scale
+    print(precision.name, "adjoint", adj_sum, "fd", fd_sum, "rel", rel, "per-ray median", np.median(per_rel),
+          "p95", np.quantile(per_rel, 0.95))
+    assert np.all(rel <= 1e-4), rel
+    assert np.quantile(per_rel, 0.95) <= 1e-4
