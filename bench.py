@@ -356,9 +356,76 @@ def run_gpu(args) -> None:
                                 "attempts_per_ray": float((d["accepted_steps"] + d["rejected_steps"]).mean()),
                                 "error_vs_oracle": comp.get(args.precision)}
         line["precision_study"] = comp
+    if args.adjoint:
+        line["adjoint"] = adjoint_study(G, args, local)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def adjoint_study(G, args, device: int) -> dict:
+    """Discrete adjoint throughput on the differentiation workload: 1024x1024 rays, a = 0.9, Q = 0.3,
+    i = 60 deg, r_obs = 50 M, MIXED forward. The loss is the sum of squared g and hit-radius residuals
+    against a target frame traced at (a, Q, i) offset by seeded N(0, 0.01) draws; one step is
+    glc_forward_ckpt + glc_backward, timed with CUDA events, for each checkpoint interval K."""
+    import numpy as np
+    import torch
+
+    n = args.adjoint_side
+    a, q, incl, r_obs = 0.9, 0.3, math.radians(60.0), 50.0
+    isco = G.prograde_isco(a, q)
+
+    def obs_at(a_, q_, i_):
+        return G.Observation.from_oblate(r_obs, i_, 0.0, spin=a_, charge=q_, chart=G.KerrSchildChart.OUTGOING,
+                                         width=n, height=n, vertical_fov=math.radians(FOV_DEG),
+                                         escape_radius=ESCAPE, surface=G.EquatorialSurface(isco, SURFACE_OUTER),
+                                         horizon_offset=HORIZON_OFFSET)
+
+    rng = np.random.default_rng(5)
+    da, dq, di = rng.normal(0.0, 0.01, 3)
+    pipe = G.TracePipeline(device, G.ReferencePolicy.frame(G.Precision.MIXED))
+    target = pipe.trace_image(obs_at(a + da, q + dq, incl + di))
+    torch.cuda.synchronize()
+    tgt = target.numpy()
+    obs = obs_at(a, q, incl)
+    stream = torch.cuda.current_stream()
+    out = {"workload": f"kerr-newman-adjoint-{n}x{n}", "spin": a, "charge": q, "inclination_deg": 60.0,
+           "observer_radius_m": r_obs, "forward_precision": "mixed", "backward_precision": "f64",
+           "target_offsets": [float(da), float(dq), float(di)], "by_K": {}}
+    for K in args.adjoint_k:
+        times = []
+        for it in range(2):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            res, tape = pipe.forward_ckpt(obs, r_obs, incl, K=K)
+            e1.record(stream)
+            d = res.numpy()
+            both = (d["termination"] == 7) & (tgt["termination"] == 7)
+            dl = np.zeros((n * n, 4))
+            dl[both, 0] = 2.0 * (d["source_radius"][both] - tgt["source_radius"][both])
+            dl[both, 1] = 2.0 * (d["frequency_ratio"][both] - tgt["frequency_ratio"][both])
+            dl_dev = torch.as_tensor(dl, device=f"cuda:{device}")
+            torch.cuda.synchronize()
+            e1b = torch.cuda.Event(enable_timing=True)
+            e1b.record(stream)
+            g = tape.backward(dl_dev, per_ray_params=False)
+            e2.record(stream)
+            torch.cuda.synchronize()
+            fwd, bwd = e0.elapsed_time(e1), e1b.elapsed_time(e2)
+            times.append((fwd, bwd))
+            info = tape.info()
+            grad = g["params"].cpu().numpy().tolist()
+            tape.close()
+        fwd, bwd = times[-1]
+        loss = float(((d["source_radius"][both] - tgt["source_radius"][both]) ** 2).sum() +
+                     ((d["frequency_ratio"][both] - tgt["frequency_ratio"][both]) ** 2).sum())
+        out["by_K"][str(K)] = {"forward_ckpt_ms": fwd, "backward_ms": bwd,
+                               "mrays_per_s": n * n / ((fwd + bwd) / 1e3) / 1e6,
+                               "checkpoint_slots": info["checkpoint_slots"], "tape_bytes": info["bytes"],
+                               "loss": loss, "dL_d(a,Q,i,r_obs)": grad}
+    out["mrays_per_s"] = max(v["mrays_per_s"] for v in out["by_K"].values())
+    pipe.close()
+    return out
 
 
 def ctypes_sizeof_job() -> int:
@@ -378,6 +445,10 @@ def main() -> None:
     ap.add_argument("--precision", choices=["fp32", "mixed", "fp64"], default="mixed")
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the discrete-adjoint throughput study (1024x1024, K = 16, 64, 256)")
+    ap.add_argument("--adjoint-side", type=int, default=1024)
+    ap.add_argument("--adjoint-k", type=int, nargs="+", default=[16, 64, 256])
     ap.add_argument("--cpu-sample", type=int, default=2048,
                     help="pixels of the frame traced by the CPU oracle (baseline and error report)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
