@@ -33,6 +33,10 @@ SPIN, CHARGE, INCL_DEG, R_OBS, FOV_DEG = 0.9, 0.3, 75.0, 50.0, 30.0
 ESCAPE, HORIZON_OFFSET, SURFACE_OUTER = 1000.0, 1e-3, 20.0
 METRIC = "Mrays/s at 3840x2160 a=0.9, mixed vs plain at equal FP64 error; adjoint Mrays/s"
 L2_BYTES = 126 * 2 ** 20
+# DRAM bytes (read + write) per ray of the trace kernel from the committed ncu captures of the same
+# scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32}_1280x720_full.md); the traffic is the
+# result store plus spill write-back, both proportional to the ray count.
+TRAFFIC_BYTES_PER_RAY = {"mixed": (9.040384e6 + 240.576256e6) / 921600, "fp32": (50.390272e6 + 991.714048e6) / 921600}
 
 
 def workload_config(precision: str, policy: dict | None = None) -> dict:
@@ -300,7 +304,11 @@ def run_gpu(args) -> None:
                 "peak_source": f"nominal {sm_count} SMs x 128 FP32 lanes x 2 x median SM clock {peak_mhz:.0f} MHz "
                                "under load (MEASURED_PEAKS.json has no FP32 figure)",
                 "alg_flops_per_launch": alg_flops, "attempted_steps": attempts,
-                "flops_per_attempt": float(flops[2]), "traffic": args.traffic_bytes}
+                "flops_per_attempt": float(flops[2]),
+                "traffic": args.traffic_bytes if args.traffic_bytes is not None else (
+                    TRAFFIC_BYTES_PER_RAY[args.precision] * rays if args.precision in TRAFFIC_BYTES_PER_RAY else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1280x720, scaled by rays",
+                "algorithmic_bytes_per_launch": 176.0 * rays}
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
