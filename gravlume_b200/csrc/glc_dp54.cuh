@@ -4,6 +4,8 @@
 // constants here, so every stage combination is an FMA with an immediate operand.
 #pragma once
 
+#include <type_traits>
+
 #include "glc_geometry.cuh"
 
 namespace glc {
@@ -70,6 +72,51 @@ template <>
 GLC_HD float dp_a<float>(int s, int j) { return kDpAf[s][j]; }
 template <>
 GLC_HD double dp_a<double>(int s, int j) { return kDpA[s][j]; }
+
+// Streaming form of the stage matrix: after the slope of stage j (0-based) is known it is added,
+// with weight kStreamA[j][m] = A[j+1+m][j], into the pending point sum of stage j+1+m; the sums
+// rotate so that the next stage's sum is always first (row 6, after the end-point slope, is zero).
+// kStreamE / kStreamB are the error weights b - b* and the fifth-order weights b per stage.
+#if defined(__CUDACC__)
+#define GLC_TABLE __constant__
+#else
+#define GLC_TABLE static const
+#endif
+#define GLC_STREAM_A(T)                                                                                  \
+  {{T(dp::a21), T(dp::a31), T(dp::a41), T(dp::a51), T(dp::a61), T(dp::b1)},                             \
+   {T(dp::a32), T(dp::a42), T(dp::a52), T(dp::a62), T(0), T(0)},                                         \
+   {T(dp::a43), T(dp::a53), T(dp::a63), T(dp::b3), T(0), T(0)},                                          \
+   {T(dp::a54), T(dp::a64), T(dp::b4), T(0), T(0), T(0)},                                                \
+   {T(dp::a65), T(dp::b5), T(0), T(0), T(0), T(0)},                                                      \
+   {T(dp::b6), T(0), T(0), T(0), T(0), T(0)},                                                            \
+   {T(0), T(0), T(0), T(0), T(0), T(0)}}
+#define GLC_STREAM_E(T) {T(dp::e1), T(0), T(dp::e3), T(dp::e4), T(dp::e5), T(dp::e6), T(dp::e7)}
+#define GLC_STREAM_B(T) {T(dp::b1), T(0), T(dp::b3), T(dp::b4), T(dp::b5), T(dp::b6), T(0)}
+GLC_TABLE float kStreamAf[7][6] = GLC_STREAM_A(float);
+GLC_TABLE double kStreamAd[7][6] = GLC_STREAM_A(double);
+GLC_TABLE float kStreamEf[7] = GLC_STREAM_E(float);
+GLC_TABLE double kStreamEd[7] = GLC_STREAM_E(double);
+GLC_TABLE float kStreamBf[7] = GLC_STREAM_B(float);
+GLC_TABLE double kStreamBd[7] = GLC_STREAM_B(double);
+#undef GLC_STREAM_A
+#undef GLC_STREAM_E
+#undef GLC_STREAM_B
+#undef GLC_TABLE
+
+template <class T>
+struct StreamCoef;
+template <>
+struct StreamCoef<float> {
+  static GLC_HD float a(int j, int m) { return kStreamAf[j][m]; }
+  static GLC_HD float e(int j) { return kStreamEf[j]; }
+  static GLC_HD float b(int j) { return kStreamBf[j]; }
+};
+template <>
+struct StreamCoef<double> {
+  static GLC_HD double a(int j, int m) { return kStreamAd[j][m]; }
+  static GLC_HD double e(int j) { return kStreamEd[j]; }
+  static GLC_HD double b(int j) { return kStreamBd[j]; }
+};
 
 struct Tolerance {
   double pos_rtol, pos_atol, mom_rtol, mom_atol;
@@ -191,6 +238,90 @@ GLC_HD C dp5_attempt_compact(const KN<C>& k, const S y0[6], C E, C h, const C k1
     num = larger ? ae : num;
     den = larger ? scale : den;
     chk += err + K[6][c];
+  }
+  finite = g_finite(chk);
+  return num * g_rcp(den);
+}
+
+// The same attempt in streaming form: all six evaluations (five interior stages and the end point)
+// run through one rolled loop around a single inlined right-hand side, whose invariants block runs
+// on the last pass only. The pending stage sums stay at fixed register positions (no local memory)
+// and the coefficients come from constant memory at the warp-uniform stage index, so the hot
+// loop's instruction footprint is about a sixth of the unrolled form's.
+// kFold: the end-point evaluation is the loop's sixth pass (one right-hand-side body; measured
+// faster in binary64) or follows the loop as its own call (measured faster in binary32).
+template <class C, class S, bool kInv = true, bool kFold = std::is_same<C, double>::value>
+GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start, const Tolerance& tol,
+                            C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite) {
+  using Coef = StreamCoef<C>;
+  C y0c[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) y0c[c] = C(y0[c]);
+  C P[6][6], err[7], bt;
+#pragma unroll
+  for (int m = 0; m < 6; ++m)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) P[m][c] = Coef::a(0, m) * k1[c];
+#pragma unroll
+  for (int c = 0; c < 7; ++c) err[c] = Coef::e(0) * k1[c];
+  bt = Coef::b(0) * k1[6];
+  C ys[6], rr = C(0), vv = C(0), d[7];
+  constexpr int kPasses = kFold ? 7 : 6;
+#pragma unroll 1
+  for (int j = 1; j < kPasses; ++j) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      if constexpr (kFold) {
+        inc[c] = h * P[0][c];
+        ys[c] = y0c[c] + inc[c];
+      } else {
+        ys[c] = y0c[c] + h * P[0][c];
+      }
+    }
+    if constexpr (kFold) {
+      kn_rhs<C, kInv>(k, ys, E, d, rr, vv, j == 6 ? &inv : nullptr);
+    } else {
+      kn_rhs<C, false>(k, ys, E, d, rr, vv);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) P[m][c] = P[m + 1][c] + Coef::a(j, m) * d[c];
+    const C ej = Coef::e(j);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) err[c] += ej * d[c];
+    bt += Coef::b(j) * d[6];
+  }
+  if constexpr (!kFold) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      inc[c] = h * P[0][c];
+      ys[c] = y0c[c] + inc[c];
+    }
+    kn_rhs<C, kInv>(k, ys, E, d, rr, vv, &inv);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) err[c] += Coef::e(6) * d[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 7; ++c) k7[c] = d[c];
+  r_end = rr;
+  vr_end = vv;
+  dt = h * bt;
+  C chk = dt + r_end;
+  if (kInv) chk += inv.lz + inv.carter;
+  C num = C(0), den = C(1);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    const C e = h * err[c];
+    const C sv = c < 6 ? y0c[c] : t_start;
+    const C ev = c < 6 ? ys[c] : t_start + dt;
+    const bool pos = c < 3 || c == 6;
+    const C scale = C(pos ? tol.pos_rtol : tol.mom_rtol) * g_max(g_abs(sv), g_abs(ev)) + C(pos ? tol.pos_atol : tol.mom_atol);
+    const C ae = g_abs(e);
+    const bool larger = ae * den > num * scale;
+    num = larger ? ae : num;
+    den = larger ? scale : den;
+    chk += e + k7[c];
   }
   finite = g_finite(chk);
   return num * g_rcp(den);

@@ -224,7 +224,7 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
   d[6] = E + fq;
   r_out = r;
   vr_out = grx * vx + gry * vy + grz * vz;
-  if (kInv) {
+  if (kInv && inv != nullptr) {
     // Carter's constant as Q = L_x^2 + L_y^2 + a^2 [(z^2/r^2)(P_perp^2 - E^2) - (rho^2/A) p_z^2]
     // (see kn_invariants): no r^2-sized terms cancel, so binary32 keeps its relative accuracy far out
     const T rho2 = x * x + yy * yy;

@@ -19,10 +19,12 @@
 
 #include <type_traits>
 
-// 1: the DP5(4) attempt runs its six stages through one rolled loop (small instruction footprint);
-// 0: fully unrolled stages.
-#ifndef GLC_COMPACT_ATTEMPT
-#define GLC_COMPACT_ATTEMPT 0
+// Form of the DP5(4) attempt: 0 fully unrolled stages; 1 one rolled loop over a stage array (local
+// memory); 2 streaming stage sums in registers around a rolled loop (dp5_attempt_stream). The
+// kernels are bound by instruction fetch, so the small footprint of form 2 wins: 3840x2160 frames
+// measured 144 -> 173 Mrays/s (binary32), 76 -> 92 (mixed), 133 -> 157 (binary64 at rtol 1e-6).
+#ifndef GLC_ATTEMPT_FORM
+#define GLC_ATTEMPT_FORM 2
 #endif
 
 #include "glc_dp54.cuh"
@@ -341,8 +343,13 @@ GLC_HD void attempt64_body(const KN<double>& kd, const double y0[6], double E, d
                            const Tolerance& tol, Attempt64* a) {
   double k1[7], rr, vv;
   kn_rhs(kd, y0, E, k1, rr, vv);
+#if GLC_ATTEMPT_FORM == 2
+  a->en = dp5_attempt_stream<double, double>(kd, y0, E, h, k1, t_start, tol, a->inc, a->dt, a->k7, a->r_end,
+                                             a->vr_end, a->inv, a->finite);
+#else
   a->en = dp5_attempt<double, double>(kd, y0, E, h, k1, t_start, tol, a->inc, a->dt, a->k7, a->r_end, a->vr_end,
                                       a->inv, a->finite);
+#endif
 }
 
 #if defined(__CUDA_ARCH__)
@@ -547,9 +554,12 @@ struct Ray {
       finite = a.finite;
     } else {
       const KN<C> kc = kn_cast<C>(sc.kn);
-#if GLC_COMPACT_ATTEMPT
+#if GLC_ATTEMPT_FORM == 1
       o.en = dp5_attempt_compact<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
                                              o.inv, finite);
+#elif GLC_ATTEMPT_FORM == 2
+      o.en = dp5_attempt_stream<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
+                                            o.inv, finite);
 #else
       o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
                                      finite);

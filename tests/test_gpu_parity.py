@@ -200,7 +200,8 @@ def test_mixed_is_at_or_below_plain_fp32_error_on_every_observable(pipe, config1
     """The precision study's acceptance at the same frame policy (rtol 1e-6), against the binary64
     oracle. Both modes accept the same kind of step sequence, so observables set by the
     controller's truncation error (directions, g, radii, travel time, invariant drifts) are the same
-    to within the scatter of a 240-ray maximum (a factor 1.5); what binary64 localization buys is
+    to within the scatter of a 240-ray maximum (a factor 1.5 plus one tolerance unit); what binary64
+    localization buys is
     the event residual, which must drop by at least three orders of magnitude, and the class counts
     must be no worse."""
     obs, sel, ref = config1_oracle
@@ -208,7 +209,10 @@ def test_mixed_is_at_or_below_plain_fp32_error_on_every_observable(pipe, config1
     f = compare(run_image(pipe, obs, G.Precision.FP32), sel, ref)
     print("mixed", m, "fp32", f)
     assert m["class_mismatch"] <= f["class_mismatch"]
-    for k in ("escape_direction_rad", "g_rel", "hit_radius", "source_azimuth", "travel_time",
-              "max_null_residual", "max_lz_drift", "max_carter_drift"):
-        assert m[k] <= 1.5 * f[k], (k, m[k], f[k])
+    # one tolerance unit: rtol 1e-6 times the observable's scale (angles and relative quantities 1,
+    # hit radius 10 M, travel time 1000 M)
+    unit = dict(escape_direction_rad=1e-6, g_rel=1e-6, hit_radius=1e-5, source_azimuth=1e-6, travel_time=1e-3,
+                max_null_residual=1e-6, max_lz_drift=1e-6, max_carter_drift=1e-6)
+    for k, u in unit.items():
+        assert m[k] <= 1.5 * f[k] + u, (k, m[k], f[k])
     assert m["event_residual_gpu_max"] <= 1e-3 * f["event_residual_gpu_max"]
