@@ -153,7 +153,9 @@ def _torch():
 
 
 class TraceResults:
-    """Caller-owned device SoA (glc_results): one 16-byte element per ray per field."""
+    """Caller-owned device SoA (glc_results): one 16-byte element per ray per field. The buffers are
+    filled with a NaN pattern on the current stream; a trace on another stream (a CUDA graph's, say)
+    must be ordered after that fill."""
 
     def __init__(self, slots: int, device, fields: Iterable[str] = N.RESULT_FIELDS, host: bool = False):
         torch = _torch()
