@@ -233,7 +233,7 @@ def run_gpu(args) -> None:
     cam = G.image_camera(0, WIDTH, HEIGHT)
     pipe = G.TracePipeline(local)
     precision = {"fp32": G.Precision.FP32, "mixed": G.Precision.MIXED, "fp64": G.Precision.FP64}[args.precision]
-    pipe.set_policy(G.ReferencePolicy.frame(precision))
+    pipe.set_policy(G.ReferencePolicy.frame(precision, persistent=int(args.persistent)))
     results = G.TraceResults(WIDTH * HEIGHT, dev)
     stream = torch.cuda.current_stream()
     if args.autotune:
@@ -422,8 +422,9 @@ def batch_job(G, seed: int = 4):
 
 def batch_study(G, device: int) -> dict:
     """The 64-scene batch plus the equirectangular escape map (batch_job) in MIXED: one persistent
-    work-queue launch, its CUDA-graph replay, the one-thread-per-ray kernel, and the launch shape
-    the autotuner picks on a 4-scene sub-job; CUDA-event time per job, L2 flushed in between."""
+    work-queue launch (lane refill), its CUDA-graph replay, the one-thread-per-ray kernel, the
+    warp-grab work queue, and the launch shape the autotuner picks on a 4-scene sub-job; CUDA-event
+    time per job, L2 flushed in between."""
     import torch
 
     scenes, cams, slots, _ = batch_job(G)
@@ -472,6 +473,10 @@ def batch_study(G, device: int) -> dict:
     pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED, persistent=0))
     ms = timed(lambda: pipe.trace(scenes, cams, res, stream=stream))
     out["simple"] = {"ms": ms, "mrays_per_s": slots / (ms / 1e3) / 1e6}
+    for grab in (64, 256):
+        pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED, persistent=2, rays_per_grab=grab))
+        ms = timed(lambda: pipe.trace(scenes, cams, res, stream=stream))
+        out[f"warp_queue_grab{grab}"] = {"ms": ms, "mrays_per_s": slots / (ms / 1e3) / 1e6}
     sub_s = scenes[:4]
     sub_c, off = [], 0
     for j in range(4):
@@ -571,6 +576,8 @@ def main() -> None:
     ap.add_argument("--precision", choices=["fp32", "mixed", "fp64"], default="mixed")
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--persistent", action="store_true",
+                    help="trace the frame with the persistent work-queue kernel instead of one thread per ray")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the discrete-adjoint throughput study (1024x1024, K = 16, 64, 256)")
     ap.add_argument("--adjoint-side", type=int, default=1024)

@@ -151,7 +151,10 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
   if (pol.persistent) {
     int per_sm = int(pol.blocks_per_sm);
     if (per_sm <= 0) {
-      GLC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<P>, int(block), 0));
+      if (pol.persistent == 2)
+        GLC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_queue_kernel<P>, int(block), 0));
+      else
+        GLC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<P>, int(block), 0));
       if (per_sm <= 0) per_sm = 1;
     }
     const unsigned long long warps_needed = (job.total + 31) / 32;
@@ -159,7 +162,10 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
     const unsigned long long grid_cap = (warps_needed * 32 + block - 1) / block;
     if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
     GLC_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream));
-    trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+    if (pol.persistent == 2)
+      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+    else
+      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
     ctx->stats.last_grid = unsigned(grid);
     ctx->stats.kernel_launches += 1;
   } else {
@@ -224,6 +230,7 @@ glc_status validate_policy(const glc_policy& p) {
   if (p.block_threads == 0 || p.block_threads % 32 != 0 || p.block_threads > 128)
     return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
   if (p.tile_w == 0 || p.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
+  if (p.persistent > 2) return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown kernel choice (persistent 0, 1 or 2)");
   return GLC_OK;
 }
 
@@ -642,7 +649,7 @@ glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
   };
   const std::vector<std::pair<uint32_t, uint32_t>> tiles = {{8, 4}, {16, 2}, {32, 1}, {4, 8}, {8, 8}, {16, 16}};
   const std::vector<Knob> knobs = {
-      {0, {0, 1}},             // persistent
+      {0, {0, 1, 2}},          // one thread per ray / lane-refill work queue / warp-grab work queue
       {1, {64, 96, 128}},      // block threads
       {2, {0, 1, 2, 3, 4, 5}}, // tile index
       {3, {32, 64, 128, 256}}, // rays per grab
@@ -663,6 +670,7 @@ glc_status glc_autotune(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
           case 5: cand.refill_min_idle = v; break;
         }
         if (!cand.persistent && k.which >= 3) continue;
+        if (cand.persistent == 2 && k.which >= 4) continue;  // no lane refill in the warp-grab queue
         float ms = 0.0f;
         s = time_policy(cand, ms);
         if (s != GLC_OK) break;

@@ -173,11 +173,11 @@ __device__ __forceinline__ bool ray_step(Ray<P>& ray, const LaneScene& ls, const
   return ray.step(ls, pol, res, P == kMIXED && use64);
 }
 
-// One thread per ray; rays in tile order so a warp covers a compact pixel tile.
+// One ray from set-up to result (the body of the one-thread-per-ray kernels).
 template <int P>
-__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out) {
+__device__ __forceinline__ void trace_one(const JobView& job, const glc_policy& pol, const glc_results& out,
+                                          unsigned long long gi) {
   using S = typename PrecTraits<P>::S;
-  const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= job.total) return;
   double st8[8], dir;
   unsigned long long slot;
@@ -198,6 +198,32 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_
     if (ray_step<P>(ray, ls, pol, res, use64)) break;
   }
   write_result<P>(out, slot, ray, res, ls);
+}
+
+// One thread per ray; rays in tile order so a warp covers a compact pixel tile.
+template <int P>
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out) {
+  trace_one<P>(job, pol, out, (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Work-queue kernel with warp-granular grabs: a grid of SMs x occupancy whose warps take
+// `rays_per_grab` consecutive rays at a time from a global atomic counter and trace them 32 at a
+// time with the one-thread-per-ray body. Load balances uneven jobs (many scenes, rays of very
+// different cost) at warp granularity without interleaving ray set-up with stepping inside a warp.
+template <int P>
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_queue_kernel(JobView job, glc_policy pol,
+                                                                                      glc_results out,
+                                                                                      unsigned long long* queue) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned grab = pol.rays_per_grab < 32u ? 32u : (pol.rays_per_grab & ~31u);
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= job.total) break;
+    for (unsigned k = 0; k < grab; k += 32u) trace_one<P>(job, pol, out, base + k + lane);
+  }
 }
 
 // Persistent kernel: every warp loops until the job's queue is drained. Idle lanes are refilled

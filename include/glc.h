@@ -133,7 +133,8 @@ typedef struct glc_policy {
   double event_affine_tolerance, event_tie_tolerance, event_arming_band, singularity_guard;
   double mixed_shell_factor;      /* MIXED: binary64 steps while r < factor * prograde photon orbit */
   uint32_t renormalize_null;      /* MIXED: renormalize the final momentum onto H = 0 */
-  uint32_t persistent;            /* 1: persistent work-queue kernel, 0: one thread per ray */
+  uint32_t persistent;            /* 0: one thread per ray; 1: persistent work queue with lane
+                                     refill; 2: persistent work queue with warp-granular grabs */
   uint32_t block_threads;         /* threads per block (multiple of 32) */
   uint32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = occupancy) */
   uint32_t tile_w, tile_h;        /* pixel tile a warp's consecutive rays cover */
