@@ -74,3 +74,55 @@ def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
         rep["equatorial_crossings_mismatch"] = int(
             (gpu["equatorial_crossings"][sel][same] != ref[same, F["equatorial_crossings"]]).sum())
     return rep
+
+
+def pinhole_states(scene, sx, sy):
+    """Initial states (t, x, y, z, p_t, p_x, p_y, p_z) of the pinhole rays through image-plane
+    points (sx, sy) (tangents of the angles along image-right and image-up), the ray set-up of the
+    trace kernels evaluated in numpy for continuous image coordinates."""
+    sx = np.atleast_1d(np.asarray(sx, dtype=np.float64))
+    sy = np.atleast_1d(np.asarray(sy, dtype=np.float64))
+    R = np.array(scene.image_right[:4]); U = np.array(scene.image_up[:4]); A = np.array(scene.arrival[:4])
+    u = np.array(scene.four_velocity[:4]); g = np.array(scene.metric_covariant[:16]).reshape(4, 4)
+    nrm = 1.0 / np.hypot(1.0, np.hypot(sx, sy))
+    sight = (np.outer(sx, R) + np.outer(sy, U) - A) * nrm[:, None]
+    pc = scene.frequency * (u - sight)
+    p = pc @ g.T
+    st = np.zeros((sx.size, 8))
+    st[:, :4] = np.array(scene.observer_txyz[:4])
+    st[:, 4:] = p
+    return st
+
+
+def near_critical_rays(pipe, spin=0.998, charge=0.05, incl_deg=85.0, r_obs=1000.0, n_dirs=128, n_rays=4096,
+                       band=0.05, seed=3, surface=True):
+    """The near-critical stress workload: the capture/escape boundary of the observer's image
+    (the critical curve) is located along n_dirs radial directions by bisection with the binary64
+    kernel at the strict policy, on the scene without its surface; then n_rays rays are drawn with
+    impact parameters uniform within +-band M of the curve at seeded directions. Returns the
+    observation (with the surface when asked), the states, and each ray's signed distance from the
+    curve in M (positive outside)."""
+    sky = config1_observation(width=64, height=64, spin=spin, charge=charge, incl_deg=incl_deg, r_obs=r_obs,
+                              escape=r_obs, surface=False)
+    sc = sky.pack()
+    pipe.set_policy(G.ReferencePolicy.strict_v1())
+    psi = np.linspace(0.0, 2 * np.pi, n_dirs, endpoint=False)
+    lo = np.zeros(n_dirs)               # captured (the image centre looks at the hole)
+    hi = np.full(n_dirs, 12.0 / r_obs)  # escapes
+    for _ in range(40):
+        mid = 0.5 * (lo + hi)
+        st = pinhole_states(sc, mid * np.cos(psi), mid * np.sin(psi))
+        d = pipe.trace_states(sky, st, direction=-1.0).numpy()
+        cap = d["termination"] == G.Termination.HORIZON_CROSSING
+        lo = np.where(cap, mid, lo)
+        hi = np.where(cap, hi, mid)
+    rc = 0.5 * (lo + hi)  # critical radius in the image plane per direction (tangent units)
+    rng = np.random.default_rng(seed)
+    k = rng.integers(0, n_dirs, n_rays)
+    t = rng.uniform(-1.0, 1.0, n_rays)
+    # impact parameter b = r_obs * rho for these tiny angles; offsets of +-band M
+    rho = rc[k] + t * band / r_obs
+    obs = config1_observation(width=64, height=64, spin=spin, charge=charge, incl_deg=incl_deg, r_obs=r_obs,
+                              escape=r_obs, surface=surface)
+    st = pinhole_states(obs.pack(), rho * np.cos(psi[k]), rho * np.sin(psi[k]))
+    return obs, st, (rho - rc[k]) * r_obs
