@@ -262,9 +262,9 @@ def run_gpu(args) -> None:
     total_ms = sum(step_ms)
     launches = pipe.stats().kernel_launches - launches0
     if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        from gravlume_b200.shard import max_over_ranks
+
+        total_ms = max_over_ranks(total_ms)
     rays = WIDTH * HEIGHT
     value = world * rays * args.steps / (total_ms / 1e3) / 1e6
     d = results.numpy()
