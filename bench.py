@@ -34,9 +34,11 @@ ESCAPE, HORIZON_OFFSET, SURFACE_OUTER = 1000.0, 1e-3, 20.0
 METRIC = "Mrays/s at 3840x2160 a=0.9, mixed vs plain at equal FP64 error; adjoint Mrays/s"
 L2_BYTES = 126 * 2 ** 20
 # DRAM bytes (read + write) per ray of the trace kernel from the committed ncu captures of the same
-# scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32}_1280x720_full.md); the traffic is the
-# result store plus spill write-back, both proportional to the ray count.
-TRAFFIC_BYTES_PER_RAY = {"mixed": (9.040384e6 + 240.576256e6) / 921600, "fp32": (50.390272e6 + 991.714048e6) / 921600}
+# scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32,fp64}_1280x720_full.md): the result
+# stores (176 B/ray, part of which the 126 MB L2 still holds when a 720p launch ends), scaled by the
+# ray count.
+TRAFFIC_BYTES_PER_RAY = {"mixed": (1.357312e6 + 116.530176e6) / 921600, "fp32": (2.645248e6 + 118.213888e6) / 921600,
+                         "fp64": (7.462912e6 + 118.290944e6) / 921600}
 
 
 def workload_config(precision: str, policy: dict | None = None) -> dict:
