@@ -362,6 +362,27 @@ def run_gpu(args) -> None:
             if ref is not None:
                 entry["error_vs_oracle"] = error_report(G, dd, ref, idx)
             comp[name] = entry
+        # tolerance sweep: throughput against error for each mode, so that modes can be compared at
+        # equal error (binary32 stepping stops improving at its rounding floor)
+        if ref is not None and args.sweep:
+            sweep = []
+            for rtol in (1e-5, 1e-6, 1e-7, 1e-8):
+                for name, prec, pair in (("fp32", G.Precision.FP32, 0), ("mixed", G.Precision.MIXED, 0),
+                                         ("mixed_pair_state", G.Precision.MIXED, 1), ("fp64", G.Precision.FP64, 0)):
+                    pipe.set_policy(G.ReferencePolicy.frame(prec, **shape, position_rtol=rtol, momentum_rtol=rtol,
+                                                            position_atol=rtol * 1e-2, momentum_atol=rtol * 1e-2,
+                                                            maximum_step=1000.0, mixed_pair_state=pair))
+                    pipe.trace([scene], [cam], results, stream=stream)
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    pipe.trace([scene], [cam], results, stream=stream)
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    ms = a.elapsed_time(b)
+                    dd = results.numpy()
+                    sweep.append({"precision": name, "rtol": rtol, "mrays_per_s": rays / (ms / 1e3) / 1e6,
+                                  "error_vs_oracle": error_report(G, dd, ref, idx)})
+            comp["tolerance_sweep"] = sweep
         comp[args.precision] = {"mrays_per_s": value / world, "ms": total_ms / args.steps,
                                 "attempts_per_ray": float((d["accepted_steps"] + d["rejected_steps"]).mean()),
                                 "error_vs_oracle": comp.get(args.precision)}
@@ -583,6 +604,8 @@ def main() -> None:
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the discrete-adjoint throughput study (1024x1024, K = 16, 64, 256)")
     ap.add_argument("--adjoint-side", type=int, default=1024)
+    ap.add_argument("--no-sweep", dest="sweep", action="store_false",
+                    help="skip the tolerance sweep of the precision study")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-scene batch study (persistent launch, graph, autotuner)")
     ap.add_argument("--adjoint-k", type=int, nargs="+", default=[16, 64, 256])
