@@ -63,6 +63,7 @@ class Policy(ctypes.Structure):
         ("blocks_per_sm", c_uint32), ("tile_w", c_uint32), ("tile_h", c_uint32),
         ("refill_interval", c_uint32), ("rays_per_grab", c_uint32),
         ("refill_min_idle", c_uint32), ("mixed_pair_state", c_uint32), ("capture_certificates", c_uint32),
+        ("escape_map", c_uint32),
     ]
 
     def as_dict(self):

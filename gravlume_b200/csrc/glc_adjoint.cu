@@ -65,9 +65,9 @@ __global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_p
   if (gi >= job.total) return;
   double st8[8], dir;
   unsigned long long slot;
-  int scene_idx;
-  bool certified;
-  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified)) {
+  int scene_idx, shortcut;
+  double rdir[3];
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) {
     meta[gi] = make_uint4(0, 0, 0, 0);
     return;
   }
@@ -106,9 +106,9 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
   if (m.w == 0u) return;
   double st8[8], dir;
   unsigned long long slot;
-  int scene_idx;
-  bool certified;
-  ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified);
+  int scene_idx, shortcut;
+  double rdir[3];
+  ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir);
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
   const KN<D9> kd = kn_dual(ls.kn);
   double wobs[kObs];
@@ -265,6 +265,8 @@ struct glc_tape {
     v.begin = reinterpret_cast<const unsigned long long*>(d_job + off_begin);
     v.cert_begin = reinterpret_cast<const unsigned long long*>(d_job + off_cert);
     v.cert = nullptr;
+    v.emap_begin = nullptr;
+    v.emap = nullptr;
     v.n_cams = 1;
     v.total = n;
     return v;

@@ -12,6 +12,7 @@
 #include "glc_context.h"
 #include "glc_internal.h"
 #include "glc_certificate.cuh"
+#include "glc_escape_map.cuh"
 
 using namespace glc;
 
@@ -56,8 +57,9 @@ size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 struct JobLayout {
   std::vector<unsigned long long> begin;
   std::vector<unsigned long long> cert_begin;  // 16x16 certificate tiles of each image camera
+  std::vector<unsigned long long> emap_begin;  // escape-map nodes of each image camera
   unsigned long long total = 0;
-  size_t off_scenes = 0, off_cams = 0, off_begin = 0, off_cert_begin = 0, bytes = 0;
+  size_t off_scenes = 0, off_cams = 0, off_begin = 0, off_cert_begin = 0, off_emap_begin = 0, bytes = 0;
 };
 
 glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cams, int32_t n_cams,
@@ -67,7 +69,8 @@ glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_cam
   if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
   L.begin.assign(size_t(n_cams) + 1, 0);
   L.cert_begin.assign(size_t(n_cams) + 1, 0);
-  unsigned long long acc = 0, tiles = 0;
+  L.emap_begin.assign(size_t(n_cams) + 1, 0);
+  unsigned long long acc = 0, tiles = 0, nodes = 0;
   for (int i = 0; i < n_cams; ++i) {
     const glc_camera& c = cams[i];
     if (c.scene_index < 0 || c.scene_index >= n_scenes)
@@ -96,17 +99,22 @@ glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_cam
     L.begin[i] = acc;
     acc += n;
     L.cert_begin[i] = tiles;
-    if (c.kind != GLC_CAMERA_RAYLIST)
+    L.emap_begin[i] = nodes;
+    if (c.kind != GLC_CAMERA_RAYLIST) {
       tiles += (unsigned long long)((c.width + kCertTile - 1) / kCertTile) * ((c.height + kCertTile - 1) / kCertTile);
+      nodes += (unsigned long long)map_grid_w(c.width) * map_grid_h(c.height);
+    }
   }
   L.begin[n_cams] = acc;
   L.cert_begin[n_cams] = tiles;
+  L.emap_begin[n_cams] = nodes;
   L.total = acc;
   L.off_scenes = 0;
   L.off_cams = align256(sizeof(glc_scene) * n_scenes);
   L.off_begin = L.off_cams + align256(sizeof(glc_camera) * n_cams);
   L.off_cert_begin = L.off_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
-  L.bytes = L.off_cert_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
+  L.off_emap_begin = L.off_cert_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
+  L.bytes = L.off_emap_begin + align256(sizeof(unsigned long long) * (n_cams + 1));
   return GLC_OK;
 }
 
@@ -116,6 +124,7 @@ void fill_staging(unsigned char* stage, const JobLayout& L, const glc_scene* sce
   std::memcpy(stage + L.off_cams, cams, sizeof(glc_camera) * n_cams);
   std::memcpy(stage + L.off_begin, L.begin.data(), sizeof(unsigned long long) * (n_cams + 1));
   std::memcpy(stage + L.off_cert_begin, L.cert_begin.data(), sizeof(unsigned long long) * (n_cams + 1));
+  std::memcpy(stage + L.off_emap_begin, L.emap_begin.data(), sizeof(unsigned long long) * (n_cams + 1));
 }
 
 JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
@@ -127,6 +136,8 @@ JobView job_view(const unsigned char* dev, const JobLayout& L, int32_t n_cams) {
   v.total = L.total;
   v.cert_begin = reinterpret_cast<const unsigned long long*>(dev + L.off_cert_begin);
   v.cert = nullptr;
+  v.emap_begin = reinterpret_cast<const unsigned long long*>(dev + L.off_emap_begin);
+  v.emap = nullptr;
   return v;
 }
 
@@ -140,6 +151,7 @@ struct glc_graph {
   unsigned char* h_stage = nullptr;
   unsigned long long* d_queue = nullptr;
   uint32_t* d_cert = nullptr;
+  uint32_t* d_emap = nullptr;
 };
 
 namespace {
@@ -186,7 +198,7 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
 // asks for certificates, else unused.
 glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, const glc_results& out,
                   cudaStream_t stream, unsigned long long* queue, uint32_t* cert = nullptr,
-                  unsigned long long cert_tiles = 0) {
+                  unsigned long long cert_tiles = 0, uint32_t* emap = nullptr, unsigned long long emap_nodes = 0) {
   if (job_in.total == 0) return GLC_OK;
   if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
     return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
@@ -196,6 +208,17 @@ glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, co
     GLC_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches += 1;
     job.cert = cert;
+  }
+  if (pol.escape_map && emap && emap_nodes > 0) {
+    const unsigned grid = unsigned((emap_nodes + 127) / 128);
+    switch (pol.precision) {
+      case GLC_FP32: escape_map_nodes_kernel<kFP32><<<grid, 128, 0, stream>>>(job, pol, out, emap); break;
+      case GLC_MIXED: escape_map_nodes_kernel<kMIXED><<<grid, 128, 0, stream>>>(job, pol, out, emap); break;
+      default: escape_map_nodes_kernel<kFP64><<<grid, 128, 0, stream>>>(job, pol, out, emap); break;
+    }
+    GLC_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+    job.emap = emap;
   }
   switch (pol.precision) {
     case GLC_FP32: return launch_precision<kFP32>(ctx, job, pol, out, stream, queue);
@@ -365,6 +388,7 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
   // at rtol 1e-7 on the 3840x2160 frame)
   p.mixed_pair_state = precision == GLC_MIXED ? 1u : 0u;
   p.capture_certificates = 0;
+  p.escape_map = 0;
   *out = p;
   return GLC_OK;
 }
@@ -429,6 +453,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->d_queue) cudaFree(ctx->d_queue);
   if (ctx->d_cert) cudaFree(ctx->d_cert);
+  if (ctx->d_emap) cudaFree(ctx->d_emap);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
@@ -489,7 +514,13 @@ glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, co
     s = ensure_cert_capacity(&ctx->d_cert, &ctx->d_cert_words, tiles);
     if (s != GLC_OK) return s;
   }
-  return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue, ctx->d_cert, tiles);
+  const unsigned long long nodes = ctx->policy.escape_map ? L.emap_begin[n_cameras] : 0ull;
+  if (nodes) {
+    s = ensure_cert_capacity(&ctx->d_emap, &ctx->d_emap_words, nodes);
+    if (s != GLC_OK) return s;
+  }
+  return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue, ctx->d_cert, tiles,
+                ctx->d_emap, nodes);
 }
 
 glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
@@ -564,13 +595,16 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
     if (G->h_stage) cudaFreeHost(G->h_stage);
     if (G->d_queue) cudaFree(G->d_queue);
     if (G->d_cert) cudaFree(G->d_cert);
+    if (G->d_emap) cudaFree(G->d_emap);
     delete G;
     return st;
   };
   const unsigned long long tiles = ctx->policy.capture_certificates ? L.cert_begin[n_cameras] : 0ull;
+  const unsigned long long nodes = ctx->policy.escape_map ? L.emap_begin[n_cameras] : 0ull;
   if (cudaMalloc(&G->d_job, L.bytes) != cudaSuccess || cudaMallocHost(&G->h_stage, L.bytes) != cudaSuccess ||
       cudaMalloc(&G->d_queue, 256) != cudaSuccess ||
-      (tiles && cudaMalloc(&G->d_cert, tiles * sizeof(uint32_t)) != cudaSuccess))
+      (tiles && cudaMalloc(&G->d_cert, tiles * sizeof(uint32_t)) != cudaSuccess) ||
+      (nodes && cudaMalloc(&G->d_emap, nodes * sizeof(uint32_t)) != cudaSuccess))
     return fail(set_error(GLC_ERR_CUDA, "graph buffer allocation failed"));
   fill_staging(G->h_stage, L, scenes, n_scenes, cameras, n_cameras);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -578,7 +612,7 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
     return fail(set_error(GLC_ERR_CUDA, "cudaStreamBeginCapture failed"));
   cudaError_t ce = cudaMemcpyAsync(G->d_job, G->h_stage, L.bytes, cudaMemcpyHostToDevice, st);
   glc_status ls = ce == cudaSuccess ? launch(ctx, job_view(G->d_job, L, n_cameras), ctx->policy, *out, st, G->d_queue,
-                                           G->d_cert, tiles)
+                                           G->d_cert, tiles, G->d_emap, nodes)
                                     : set_error(GLC_ERR_CUDA, cudaGetErrorString(ce));
   cudaGraph_t gr = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(st, &gr);
@@ -612,6 +646,7 @@ glc_status glc_graph_destroy(glc_graph* graph) {
   if (graph->h_stage) cudaFreeHost(graph->h_stage);
   if (graph->d_queue) cudaFree(graph->d_queue);
   if (graph->d_cert) cudaFree(graph->d_cert);
+  if (graph->d_emap) cudaFree(graph->d_emap);
   delete graph;
   return GLC_OK;
 }

@@ -17,16 +17,120 @@ struct JobView {
   unsigned long long total;
   const unsigned long long* cert_begin;  // n_cams + 1 entries: first 16x16-tile word of each camera
   const uint32_t* cert;                  // per-tile capture certificates, or null when not evaluated
+  const unsigned long long* emap_begin;  // n_cams + 1 entries: first escape-map node of each camera
+  const uint32_t* emap;                  // packed escape-map nodes, or null when not traced
 };
+
+// ---- escape-direction map (crates/gravlume-render/src/shaders/geodesic_acceleration.wgsl:330-586)
+// Nodes sit on every 4th pixel of each axis; 8x8 pixel tiles see a 3x3 stencil of nodes. A node is
+// packed into 32 bits like the reference's map: tag << 30 (1 escape, 2 horizon, 0 anything else)
+// and, for escapes, the octahedral projection of the unit escape direction in 15 + 15 bits.
+constexpr uint32_t kMapNodeStep = 4, kMapTile = 8, kMapTagShift = 30, kMapTagEscape = 1, kMapTagHorizon = 2;
+constexpr uint32_t kMapOctMax = 0x7fffu;
+constexpr double kMapMaxStencilError = 3.0e-4;  // room inside the 3.82e-4 rad direction budget
+
+__host__ __device__ __forceinline__ uint32_t map_grid_w(uint32_t w) { return 2u * ((w + kMapTile - 1) / kMapTile) + 1u; }
+__host__ __device__ __forceinline__ uint32_t map_grid_h(uint32_t h) { return 2u * ((h + kMapTile - 1) / kMapTile) + 1u; }
+
+__device__ __forceinline__ float oct_sign(float v) { return v >= 0.0f ? 1.0f : -1.0f; }
+
+__device__ __forceinline__ uint32_t map_pack_escape(double dx, double dy, double dz) {
+  const double l1 = fabs(dx) + fabs(dy) + fabs(dz);
+  if (!(l1 > 0.0) || !isfinite(l1)) return 0u;
+  float px = float(dx / l1), py = float(dy / l1);
+  if (dz < 0.0) {
+    const float qx = (1.0f - fabsf(py)) * oct_sign(px), qy = (1.0f - fabsf(px)) * oct_sign(py);
+    px = qx;
+    py = qy;
+  }
+  const float ex = fminf(fmaxf(0.5f * px + 0.5f, 0.0f), 1.0f), ey = fminf(fmaxf(0.5f * py + 0.5f, 0.0f), 1.0f);
+  const uint32_t ux = uint32_t(rintf(ex * float(kMapOctMax))), uy = uint32_t(rintf(ey * float(kMapOctMax)));
+  return ux | (uy << 15) | (kMapTagEscape << kMapTagShift);
+}
+
+// Unpacked node: tag and unit direction (escapes only).
+__device__ __forceinline__ uint32_t map_unpack(uint32_t packed, float d[3]) {
+  const uint32_t tag = packed >> kMapTagShift;
+  d[0] = d[1] = d[2] = 0.0f;
+  if (tag != kMapTagEscape) return tag;
+  float px = 2.0f * float(packed & kMapOctMax) / float(kMapOctMax) - 1.0f;
+  float py = 2.0f * float((packed >> 15) & kMapOctMax) / float(kMapOctMax) - 1.0f;
+  const float z = 1.0f - fabsf(px) - fabsf(py);
+  if (z < 0.0f) {
+    const float qx = (1.0f - fabsf(py)) * oct_sign(px), qy = (1.0f - fabsf(px)) * oct_sign(py);
+    px = qx;
+    py = qy;
+  }
+  const float n = rsqrtf(px * px + py * py + z * z);
+  d[0] = px * n;
+  d[1] = py * n;
+  d[2] = z * n;
+  return tag;
+}
+
+__device__ __forceinline__ void map_bilerp(const float a[3], const float b[3], const float c[3], const float e[3],
+                                           float u, float v, float out[3]) {
+  float n2 = 0.0f;
+  for (int i = 0; i < 3; ++i) {
+    const float top = a[i] + (b[i] - a[i]) * u, bot = c[i] + (e[i] - c[i]) * u;
+    out[i] = top + (bot - top) * v;
+    n2 += out[i] * out[i];
+  }
+  const float n = rsqrtf(n2);
+  for (int i = 0; i < 3; ++i) out[i] *= n;
+}
+
+// Escape direction of pixel (px, py) reconstructed from its tile's 3x3 stencil, when the tile is
+// stable: all nine nodes escaped and the five inner nodes lie within min(half a pixel, 3e-4 rad)
+// of the bilinear interpolation of the four corners (escape_map_tile_is_stable). Returns false
+// otherwise.
+__device__ inline bool map_reconstruct(const uint32_t* nodes, uint32_t gw, uint32_t px, uint32_t py,
+                                       double half_pixel, double dir[3]) {
+  const uint32_t tx = px / kMapTile, ty = py / kMapTile;
+  float st[9][3];
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      const uint32_t packed = nodes[(2u * ty + uint32_t(j)) * gw + 2u * tx + uint32_t(i)];
+      if (map_unpack(packed, st[3 * j + i]) != kMapTagEscape) return false;
+    }
+  const float tol = float(fmin(half_pixel, kMapMaxStencilError));
+  const float tol2 = tol * tol;
+  // inner nodes (1, 3, 4, 5, 7) at tile coordinates (1/2, 0), (0, 1/2), (1/2, 1/2), (1, 1/2), (1/2, 1)
+  const int inner[5] = {1, 3, 4, 5, 7};
+  const float iu[5] = {0.5f, 0.0f, 0.5f, 1.0f, 0.5f}, iv[5] = {0.0f, 0.5f, 0.5f, 0.5f, 1.0f};
+  for (int k = 0; k < 5; ++k) {
+    float pr[3];
+    map_bilerp(st[0], st[2], st[6], st[8], iu[k], iv[k], pr);
+    const float dx = pr[0] - st[inner[k]][0], dy = pr[1] - st[inner[k]][1], dz = pr[2] - st[inner[k]][2];
+    const float e2 = dx * dx + dy * dy + dz * dz;
+    if (!(e2 <= tol2)) return false;
+  }
+  // the pixel's 2x2 sub-cell of the stencil
+  const uint32_t lx = px - tx * kMapTile, ly = py - ty * kMapTile;
+  const uint32_t cx = min(lx / kMapNodeStep, 1u), cy = min(ly / kMapNodeStep, 1u);
+  const float u = float(lx - cx * kMapNodeStep) / float(kMapNodeStep);
+  const float v = float(ly - cy * kMapNodeStep) / float(kMapNodeStep);
+  const int f = int(cy * 3u + cx);
+  float d[3];
+  map_bilerp(st[f], st[f + 1], st[f + 3], st[f + 4], u, v, d);
+  for (int i = 0; i < 3; ++i) dir[i] = double(d[i]);
+  return true;
+}
+
+// Ways a ray of an image camera can be settled without its own integration.
+enum RayShortcut : int { kShortNone = 0, kShortCertified = 1, kShortMapNode = 2, kShortReconstructed = 3 };
 
 // Initial state of ray gi of the job. Image rays are generated in binary64 from the camera basis
 // (scene.rs:211-270, view.rs:408-424): sight = (s_x right + s_y up - arrival) / |.|,
 // p^mu = omega (u^mu - sight^mu), p_mu = g_{mu nu} p^nu at the observer. Returns false for tile
 // padding outside the image.
+__device__ __forceinline__ void image_state(const glc_scene* sc, const glc_camera* cam, uint32_t px, uint32_t py,
+                                            double st8[8]);
+
 __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& pol, unsigned long long gi,
                                           double st8[8], double& dir, unsigned long long& slot, int& scene_idx,
-                                          bool& certified) {
-  certified = false;
+                                          int& shortcut, double rdir[3]) {
+  shortcut = kShortNone;
   int lo = 0, hi = job.n_cams - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -62,11 +166,34 @@ __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& 
   if (job.cert) {
     const unsigned long long t = job.cert_begin[lo] + (unsigned long long)(py >> 4) * ((W + 15u) >> 4) + (px >> 4);
     if (job.cert[t]) {
-      certified = true;
+      shortcut = kShortCertified;
       return true;
     }
   }
   const glc_scene* sc = job.scenes + scene_idx;
+  if (job.emap) {
+    // node pixels were traced by the node pass; stable tiles take the interpolated direction
+    if (px % kMapNodeStep == 0u && py % kMapNodeStep == 0u) {
+      shortcut = kShortMapNode;
+      return true;
+    }
+    if (!sc->has_surface) {
+      const double half_pixel = cam->kind == GLC_CAMERA_PINHOLE ? sc->tangent_half_fov / double(H)
+                                                                : 0.5 * 3.141592653589793 / double(H);
+      if (map_reconstruct(job.emap + job.emap_begin[lo], map_grid_w(W), px, py, half_pixel, rdir)) {
+        shortcut = kShortReconstructed;
+        return true;
+      }
+    }
+  }
+  image_state(sc, cam, px, py, st8);
+  return true;
+}
+
+// Initial state of pixel (px, py) of an image camera (pinhole sight plane or equirectangular map).
+__device__ __forceinline__ void image_state(const glc_scene* sc, const glc_camera* cam, uint32_t px, uint32_t py,
+                                            double st8[8]) {
+  const uint32_t W = cam->width, H = cam->height;
   double sight[4];
   if (cam->kind == GLC_CAMERA_PINHOLE) {
     const double w = double(W), h = double(H);
@@ -101,7 +228,6 @@ __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& 
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) st8[i] = sc->observer_txyz[i];
-  return true;
 }
 
 template <int P>
@@ -131,15 +257,35 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
   }
 }
 
-// A ray of a certified tile: horizon capture proven without integration (flag bit 2, code bit
-// 22); the integration observables are NaN and the counters zero.
+// A ray of a certified tile: horizon capture proven without integration (kFlagCertified); the
+// integration observables are NaN and the counters zero.
 __device__ __forceinline__ void write_certified(const glc_results& o, unsigned long long slot) {
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
-  const uint32_t code = uint32_t(GLC_TERM_HORIZON) | (1u << 16) | (4u << 20);
+  const uint32_t code = uint32_t(GLC_TERM_HORIZON) | (1u << 16) | (uint32_t(kFlagCertified) << 20);
   if (o.code) reinterpret_cast<uint4*>(o.code)[slot] = make_uint4(code, 0u, 0u, 0u);
   if (o.branch) reinterpret_cast<int4*>(o.branch)[slot] = make_int4(0, 0, 0, 0);
   const double2 nn = make_double2(nan, nan);
   if (o.escape) reinterpret_cast<double2*>(o.escape)[slot] = nn;
+  if (o.surface) reinterpret_cast<double2*>(o.surface)[slot] = nn;
+  if (o.redshift_time) reinterpret_cast<double2*>(o.redshift_time)[slot] = nn;
+  if (o.event) reinterpret_cast<double2*>(o.event)[slot] = nn;
+  if (o.drift_a) reinterpret_cast<double2*>(o.drift_a)[slot] = make_double2(0.0, 0.0);
+  if (o.drift_b) reinterpret_cast<double2*>(o.drift_b)[slot] = make_double2(0.0, 0.0);
+  if (o.turning) reinterpret_cast<double2*>(o.turning)[slot] = nn;
+  if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = nn;
+  if (o.position_zr) reinterpret_cast<double2*>(o.position_zr)[slot] = nn;
+}
+
+// A ray of a stable escape-map tile: an escape whose direction is interpolated from the tile's
+// nodes (kFlagReconstructed); the other observables are NaN and the counters zero.
+__device__ __forceinline__ void write_reconstructed(const glc_results& o, unsigned long long slot, const double d[3]) {
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  const uint32_t code = uint32_t(GLC_TERM_ESCAPE) | (1u << 16) | (uint32_t(kFlagReconstructed) << 20);
+  if (o.code) reinterpret_cast<uint4*>(o.code)[slot] = make_uint4(code, 0u, 0u, 0u);
+  if (o.branch) reinterpret_cast<int4*>(o.branch)[slot] = make_int4(0, 0, 0, 0);
+  const double2 nn = make_double2(nan, nan);
+  const double cz = fmin(fmax(d[2], -1.0), 1.0);
+  if (o.escape) reinterpret_cast<double2*>(o.escape)[slot] = make_double2(acos(cz), atan2(d[1], d[0]));
   if (o.surface) reinterpret_cast<double2*>(o.surface)[slot] = nn;
   if (o.redshift_time) reinterpret_cast<double2*>(o.redshift_time)[slot] = nn;
   if (o.event) reinterpret_cast<double2*>(o.event)[slot] = nn;
@@ -181,11 +327,12 @@ __device__ __forceinline__ void trace_one(const JobView& job, const glc_policy& 
   if (gi >= job.total) return;
   double st8[8], dir;
   unsigned long long slot;
-  int scene_idx;
-  bool certified;
-  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, certified)) return;
-  if (certified) {
-    write_certified(out, slot);
+  int scene_idx, shortcut;
+  double rdir[3];
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) return;
+  if (shortcut != kShortNone) {
+    if (shortcut == kShortCertified) write_certified(out, slot);
+    else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
     return;
   }
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
@@ -272,12 +419,12 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
         const unsigned rank = __popc(idle & lt_mask);
         const bool mine = ((idle >> lane) & 1u) && rank < take;
         if (mine) {
-          double st8[8], dir;
-          int scene_idx;
-          bool certified;
-          if (ray_setup(job, pol, grab_next + rank, st8, dir, slot, scene_idx, certified)) {
-            if (certified) {
-              write_certified(out, slot);
+          double st8[8], dir, rdir[3];
+          int scene_idx, shortcut;
+          if (ray_setup(job, pol, grab_next + rank, st8, dir, slot, scene_idx, shortcut, rdir)) {
+            if (shortcut != kShortNone) {
+              if (shortcut == kShortCertified) write_certified(out, slot);
+              else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
             } else {
               ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
               ray.init(ls, pol, st8, dir);

@@ -181,8 +181,10 @@ extern "C" glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t 
   job.begin = reinterpret_cast<const unsigned long long*>(job_dev + off_begin);
   job.n_cams = n_cameras;
   job.total = acc;
-  job.cert_begin = nullptr;  // no certificate buffer without a context: every ray is integrated
-  job.cert = nullptr;
+  job.cert_begin = nullptr;  // no certificate or escape-map buffers without a context: every ray
+  job.cert = nullptr;        // is integrated
+  job.emap_begin = nullptr;
+  job.emap = nullptr;
   switch (pol.precision) {
     case GLC_FP32: return launch_static<kFP32>(device, job, pol, *out, st, queue);
     case GLC_MIXED: return launch_static<kMIXED>(device, job, pol, *out, st, queue);

@@ -59,6 +59,8 @@ enum FlagBit : uint32_t {
   kFlagRenormalized = 1u << 1, // MIXED: final momentum renormalized onto H = 0
   kFlagSurfaceInvalid = 1u << 2,  // surface hit but the circular emitter observable is undefined
   kFlagNoEscapeDirection = 1u << 3,
+  kFlagCertified = 1u << 4,       // horizon capture proven by the tile's interval certificate
+  kFlagReconstructed = 1u << 5,   // escape direction reconstructed from the escape-direction map
 };
 
 struct CompSum {

@@ -144,6 +144,8 @@ typedef struct glc_policy {
   uint32_t mixed_pair_state;      /* MIXED: accumulate the state as compensated binary32 pairs */
   uint32_t capture_certificates;  /* 1: interval capture certificates on 16x16 tiles of image
                                      cameras of surface-free scenes; certified rays skip integration */
+  uint32_t escape_map;            /* 1: escape-direction map (node pass on every 4th pixel, stable
+                                     8x8 tiles of surface-free scenes reconstructed by interpolation) */
 } glc_policy;
 
 typedef enum glc_camera_kind {
@@ -167,7 +169,9 @@ typedef struct glc_camera {
  * pointer may be NULL to skip that field. Lengths: >= max(result_offset + rays of camera).
  *   code.x  termination | failure << 8 | event candidates << 12 | (polar side + 1) << 16
  *           | flags << 20 (bit 20: shell steps taken in binary64; bit 21: null renormalized;
- *           bit 22: capture proven by the tile's interval certificate, ray not integrated)
+ *           bit 22: surface hit whose emitter observable is undefined; bit 23: escape without a
+ *           direction; bit 24: capture proven by the tile's interval certificate, ray not
+ *           integrated; bit 25: escape direction reconstructed from the escape-direction map)
  *   code.y  accepted steps, code.z rejected steps, code.w binary64 steps (MIXED)
  *   branch  radial turnings, equatorial crossings, azimuth winding, has turning radius
  *   escape  (polar angle, azimuth) of the unit coordinate direction at escape (NaN otherwise)

@@ -19,7 +19,7 @@ from gpu_common import config1_observation, oracle_for
 
 pytestmark = pytest.mark.gpu
 
-CERTIFIED = 4  # bit 22 of code.x, i.e. bit 2 of the decoded flags
+CERTIFIED = 16  # bit 24 of code.x, i.e. bit 4 of the decoded flags
 
 
 @pytest.fixture(scope="module")
