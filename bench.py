@@ -35,7 +35,7 @@ METRIC = "Mrays/s at 3840x2160 a=0.9, mixed vs plain at equal FP64 error; adjoin
 L2_BYTES = 126 * 2 ** 20
 # DRAM bytes (read + write) per ray of the trace kernel from the committed ncu captures of the same
 # scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32,fp64}_1280x720_full.md): the result
-# stores (176 B/ray, part of which the 126 MB L2 still holds when a 720p launch ends), scaled by the
+# stores (200 B/ray, part of which the 126 MB L2 still holds when a 720p launch ends), scaled by the
 # ray count.
 TRAFFIC_BYTES_PER_RAY = {"mixed": (1.357312e6 + 116.530176e6) / 921600, "fp32": (2.645248e6 + 118.213888e6) / 921600,
                          "fp64": (7.462912e6 + 118.290944e6) / 921600}
@@ -47,7 +47,7 @@ def workload_config(precision: str, policy: dict | None = None) -> dict:
         "charge": CHARGE, "inclination_deg": INCL_DEG, "observer_radius_m": R_OBS, "vertical_fov_deg": FOV_DEG,
         "escape_radius_m": ESCAPE, "capture": "r_+ + 1e-3", "surface": "prograde ISCO .. 20 M", "chart": "outgoing",
         "precision": precision, "stepper": "DP5(4) adaptive",
-        "l2": "L2 flushed between timed frames (256 MiB write); results 1.46 GB/frame exceed L2",
+        "l2": "L2 flushed between timed frames (256 MiB write); results 1.66 GB/frame exceed L2",
     }
     if policy:
         cfg["policy"] = policy
@@ -283,7 +283,8 @@ def run_gpu(args) -> None:
         N.check(N.lib().glc_trace_host(pipe._h, sa, 1, ca, 1, rs), "glc_trace_host")
     e2e_ms = 1e3 * (time.perf_counter() - t0) / e2e_steps
     e2e = {"value": rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
-           "h2d_bytes_per_step": int(ctypes_sizeof_job()), "d2h_bytes_per_step": int(WIDTH * HEIGHT * 16 * 11)}
+           "h2d_bytes_per_step": int(ctypes_sizeof_job()),
+           "d2h_bytes_per_step": int(WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
 
     if rank != 0:
         if dist:
@@ -310,7 +311,7 @@ def run_gpu(args) -> None:
                 "traffic": args.traffic_bytes if args.traffic_bytes is not None else (
                     TRAFFIC_BYTES_PER_RAY[args.precision] * rays if args.precision in TRAFFIC_BYTES_PER_RAY else None),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1280x720, scaled by rays",
-                "algorithmic_bytes_per_launch": 176.0 * rays}
+                "algorithmic_bytes_per_launch": float(sum(N.RESULT_BYTES.values())) * rays}
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,

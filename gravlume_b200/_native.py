@@ -11,6 +11,7 @@ c_double, c_int32, c_uint32, c_uint64, c_void_p = (ctypes.c_double, ctypes.c_int
                                                    ctypes.c_uint64, ctypes.c_void_p)
 
 GLC_OK = 0
+ABI_VERSION = 2  # GLC_ABI_VERSION of include/glc.h these structures mirror
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "NON_FINITE", 4: "NON_POSITIVE",
     5: "NON_NORMALIZED", 6: "EXTREMALITY_CHANGED", 7: "NON_STATIONARY", 8: "DEGENERATE_FRAME",
@@ -30,6 +31,8 @@ class SceneInput(ctypes.Structure):
         ("width", c_uint32), ("height", c_uint32), ("vertical_fov", c_double),
         ("escape_radius", c_double), ("surface_inner", c_double), ("surface_outer", c_double),
         ("intensity_at_six", c_double), ("horizon_offset", c_double),
+        ("emission_model", c_int32), ("has_slab", c_int32), ("temperature_at_six", c_double),
+        ("slab_optical_depth", c_double), ("slab_emission", c_double), ("slab_temperature", c_double),
     ]
 
 
@@ -45,7 +48,9 @@ class Scene(ctypes.Structure):
         ("metric_covariant", c_double * 16), ("frequency", c_double),
         ("tangent_half_fov", c_double), ("width", c_uint32), ("height", c_uint32),
         ("extremality", c_int32), ("has_horizon", c_int32), ("has_escape", c_int32),
-        ("has_surface", c_int32), ("reserved", c_int32 * 2),
+        ("has_surface", c_int32), ("emission_model", c_int32), ("reserved", c_int32),
+        ("temperature_at_six", c_double), ("slab_transmittance", c_double), ("slab_emission", c_double),
+        ("slab_bands", c_double * 3),
     ]
 
 
@@ -79,7 +84,9 @@ class Camera(ctypes.Structure):
 
 
 RESULT_FIELDS = ["code", "branch", "escape", "surface", "redshift_time", "event", "drift_a",
-                 "drift_b", "turning", "position_xy", "position_zr"]
+                 "drift_b", "turning", "position_xy", "position_zr", "intensity", "radiance"]
+# bytes per ray of each result field (radiance is RGBA16F)
+RESULT_BYTES = {name: 16 for name in RESULT_FIELDS} | {"radiance": 8}
 
 
 class Results(ctypes.Structure):
@@ -157,6 +164,8 @@ def lib(path: Path | None = None):
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        if L.glc_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{p} has ABI {L.glc_abi_version()}, the bindings expect {ABI_VERSION}: rebuild it")
         _lib = L
     return _lib
 

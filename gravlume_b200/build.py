@@ -19,7 +19,7 @@ LIB_PATH = LIB_DIR / "libglc.so"
 
 SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_adjoint.cu", "glc_scene.cpp", "glc_flops.cpp"]
 HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh", "glc_escape_map.cuh",
-           "glc_dual.cuh", "glc_adjoint.cuh", "glc_internal.h", "glc_context.h"]
+           "glc_dual.cuh", "glc_adjoint.cuh", "glc_radiation.cuh", "glc_internal.h", "glc_context.h"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

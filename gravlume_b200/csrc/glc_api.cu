@@ -530,10 +530,14 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
   uint64_t slots = 0;
   glc_status s = glc_result_slots(scenes, n_scenes, cameras, n_cameras, &slots);
   if (s != GLC_OK) return s;
-  void* hfields[11] = {host_out->code,    host_out->branch,  host_out->escape,      host_out->surface,
-                       host_out->redshift_time, host_out->event, host_out->drift_a, host_out->drift_b,
-                       host_out->turning, host_out->position_xy, host_out->position_zr};
-  // workspace layout: ray-list states, then one 16-byte-per-slot array per requested field
+  constexpr int kFields = 13;
+  void* hfields[kFields] = {host_out->code,    host_out->branch,  host_out->escape,      host_out->surface,
+                            host_out->redshift_time, host_out->event, host_out->drift_a, host_out->drift_b,
+                            host_out->turning, host_out->position_xy, host_out->position_zr, host_out->intensity,
+                            host_out->radiance};
+  // bytes per slot of each field (radiance is RGBA16F)
+  const size_t esize[kFields] = {16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 8};
+  // workspace layout: ray-list states, then one array per requested field
   std::vector<size_t> state_off(size_t(n_cameras), 0);
   size_t bytes = 0;
   for (int i = 0; i < n_cameras; ++i)
@@ -541,10 +545,10 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
       state_off[i] = bytes;
       bytes += align256(cameras[i].n_rays * 8 * sizeof(double));
     }
-  size_t field_off[11];
-  for (int i = 0; i < 11; ++i) {
+  size_t field_off[kFields];
+  for (int i = 0; i < kFields; ++i) {
     field_off[i] = bytes;
-    if (hfields[i]) bytes += align256(slots * 16);
+    if (hfields[i]) bytes += align256(slots * esize[i]);
   }
   if (bytes > ctx->d_host_ws_bytes) {
     if (ctx->d_host_ws) GLC_CUDA(cudaFree(ctx->d_host_ws));
@@ -563,15 +567,16 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     }
   }
   glc_results dev{};
-  void** dfields[11] = {(void**)&dev.code,    (void**)&dev.branch,  (void**)&dev.escape,      (void**)&dev.surface,
-                        (void**)&dev.redshift_time, (void**)&dev.event, (void**)&dev.drift_a, (void**)&dev.drift_b,
-                        (void**)&dev.turning, (void**)&dev.position_xy, (void**)&dev.position_zr};
-  for (int i = 0; i < 11; ++i) *dfields[i] = hfields[i] ? ctx->d_host_ws + field_off[i] : nullptr;
+  void** dfields[kFields] = {(void**)&dev.code,    (void**)&dev.branch,  (void**)&dev.escape,  (void**)&dev.surface,
+                             (void**)&dev.redshift_time, (void**)&dev.event, (void**)&dev.drift_a,
+                             (void**)&dev.drift_b, (void**)&dev.turning, (void**)&dev.position_xy,
+                             (void**)&dev.position_zr, (void**)&dev.intensity, (void**)&dev.radiance};
+  for (int i = 0; i < kFields; ++i) *dfields[i] = hfields[i] ? ctx->d_host_ws + field_off[i] : nullptr;
   s = glc_trace(ctx, scenes, n_scenes, cams.data(), n_cameras, &dev, nullptr);
   if (s != GLC_OK) return s;
-  for (int i = 0; i < 11; ++i) {
+  for (int i = 0; i < kFields; ++i) {
     if (!hfields[i]) continue;
-    GLC_CUDA(cudaMemcpyAsync(hfields[i], *dfields[i], slots * 16, cudaMemcpyDeviceToHost, nullptr));
+    GLC_CUDA(cudaMemcpyAsync(hfields[i], *dfields[i], slots * esize[i], cudaMemcpyDeviceToHost, nullptr));
   }
   GLC_CUDA(cudaStreamSynchronize(nullptr));
   return GLC_OK;

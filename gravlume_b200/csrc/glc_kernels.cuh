@@ -2,6 +2,7 @@
 // persistent work-queue kernel with warp-level refill of finished lanes.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "glc_tracer.cuh"
@@ -230,6 +231,27 @@ __device__ __forceinline__ void image_state(const glc_scene* sc, const glc_camer
   for (int i = 0; i < 4; ++i) st8[i] = sc->observer_txyz[i];
 }
 
+// Binary16 bits of a non-negative intensity, saturating at the largest finite binary16.
+__device__ __forceinline__ unsigned short half_bits(double v) {
+  const float f = v > 65504.0 ? 65504.0f : (v > 0.0 ? float(v) : 0.0f);
+  return __half_as_ushort(__float2half_rn(f));
+}
+
+// intensity and radiance stores of one ray (surface transport; zero radiance elsewhere)
+__device__ __forceinline__ void write_radiance(const glc_results& o, unsigned long long slot, double emitted,
+                                               double observed, const double rgb[3]) {
+  const bool hit = isfinite(observed);
+  if (o.intensity)
+    reinterpret_cast<double2*>(o.intensity)[slot] =
+        hit ? make_double2(observed, emitted) : make_double2(__longlong_as_double(0x7ff8000000000000ll),
+                                                             __longlong_as_double(0x7ff8000000000000ll));
+  if (o.radiance) {
+    ushort4 v = make_ushort4(0, 0, 0, 0);
+    if (hit) v = make_ushort4(half_bits(rgb[0]), half_bits(rgb[1]), half_bits(rgb[2]), half_bits(2.0));
+    reinterpret_cast<ushort4*>(o.radiance)[slot] = v;
+  }
+}
+
 template <int P>
 __device__ __forceinline__ void write_result(const glc_results& o, unsigned long long slot, const Ray<P>& ray,
                                              const RayResult<typename PrecTraits<P>::S>& res, const LaneScene& ls) {
@@ -255,6 +277,7 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
     const double r = kn_radius(ls.kn, double(ray.ys(0)), double(ray.ys(1)), double(ray.ys(2)), gs);
     reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(ray.ys(2)), r);
   }
+  write_radiance(o, slot, res.emitted, res.observed, res.rgb);
 }
 
 // A ray of a certified tile: horizon capture proven without integration (kFlagCertified); the
@@ -274,6 +297,8 @@ __device__ __forceinline__ void write_certified(const glc_results& o, unsigned l
   if (o.turning) reinterpret_cast<double2*>(o.turning)[slot] = nn;
   if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = nn;
   if (o.position_zr) reinterpret_cast<double2*>(o.position_zr)[slot] = nn;
+  const double none[3] = {0.0, 0.0, 0.0};
+  write_radiance(o, slot, nan, nan, none);
 }
 
 // A ray of a stable escape-map tile: an escape whose direction is interpolated from the tile's
@@ -294,6 +319,8 @@ __device__ __forceinline__ void write_reconstructed(const glc_results& o, unsign
   if (o.turning) reinterpret_cast<double2*>(o.turning)[slot] = nn;
   if (o.position_xy) reinterpret_cast<double2*>(o.position_xy)[slot] = nn;
   if (o.position_zr) reinterpret_cast<double2*>(o.position_zr)[slot] = nn;
+  const double none[3] = {0.0, 0.0, 0.0};
+  write_radiance(o, slot, nan, nan, none);
 }
 
 // Register budget per precision: binary32 fits 128 registers (16 warps per SM); the binary64 and

@@ -15,6 +15,7 @@
 #include <limits>
 
 #include "glc_internal.h"
+#include "glc_radiation.cuh"
 
 namespace glc {
 
@@ -285,6 +286,36 @@ glc_status pack_scene(const glc_scene_input& in, glc_scene& out) {
   out.surface_inner = in.has_surface ? in.surface_inner / M : 0.0;
   out.surface_outer = in.has_surface ? in.surface_outer / M : 0.0;
   out.intensity_at_six = in.has_surface ? in.intensity_at_six : 0.0;
+  // surface emission and transport (EquatorialEmissionModel, SurfaceTransport)
+  out.emission_model = 0;
+  out.reserved = 0;
+  out.temperature_at_six = 0.0;
+  out.slab_transmittance = 1.0;
+  out.slab_emission = 0.0;
+  out.slab_bands[0] = out.slab_bands[1] = out.slab_bands[2] = 0.0;
+  if (in.has_surface) {
+    if (in.emission_model != 0 && in.emission_model != 1)
+      return set_error(GLC_ERR_INVALID_SURFACE, "unknown surface emission model");
+    out.emission_model = in.emission_model;
+    if (in.emission_model == 1) {
+      if (!std::isfinite(in.temperature_at_six) || !(in.temperature_at_six > 0.0))
+        return set_error(GLC_ERR_INVALID_SURFACE, "blackbody temperature at 6 M must be finite and positive");
+      out.temperature_at_six = in.temperature_at_six;
+    }
+    if (in.has_slab) {
+      if (!std::isfinite(in.slab_optical_depth) || in.slab_optical_depth < 0.0 || !std::isfinite(in.slab_emission) ||
+          in.slab_emission < 0.0)
+        return set_error(GLC_ERR_INVALID_SURFACE, "slab optical depth and emission must be finite and non-negative");
+      out.slab_transmittance = std::exp(-in.slab_optical_depth);
+      out.slab_emission = in.slab_emission;
+      if (in.emission_model == 1 && in.slab_emission > 0.0) {
+        if (!std::isfinite(in.slab_temperature) || !(in.slab_temperature > 0.0))
+          return set_error(GLC_ERR_INVALID_SURFACE, "slab temperature must be finite and positive");
+        if (!blackbody_bands(in.slab_emission, in.slab_temperature, out.slab_bands))
+          return set_error(GLC_ERR_INVALID_SURFACE, "slab spectrum is not representable");
+      }
+    }
+  }
   // inner (prograde) circular photon orbit: the MIXED binary64 shell r < factor * r_ph hugs the
   // horizon and the co-rotating photon sphere
   out.photon_shell_radius = photon_orbit(a, q, +1.0);

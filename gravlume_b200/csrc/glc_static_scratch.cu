@@ -26,8 +26,8 @@ using namespace glc;
 namespace {
 
 // Scratch size: 256 bytes for the queue counter, the rest for the job table (scenes, cameras and
-// per-camera ray offsets, each section 256-byte aligned). 64 KiB holds 128 scenes and 128 cameras.
-constexpr size_t kScratchBytes = 64 * 1024;
+// per-camera ray offsets, each section 256-byte aligned). 96 KiB holds 128 scenes and 128 cameras.
+constexpr size_t kScratchBytes = 96 * 1024;
 constexpr size_t kQueueBytes = 256;
 constexpr int kMaxScenes = 128;
 constexpr int kMaxCameras = 128;
@@ -118,7 +118,7 @@ extern "C" glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t 
   if (n_scenes <= 0 || n_cameras <= 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "scenes and cameras must be non-empty");
   if (n_scenes > kMaxScenes || n_cameras > kMaxCameras)
     return set_error(GLC_ERR_CAPACITY,
-                     "glc_trace_static_scratch takes at most 128 scenes and 128 cameras (64 KiB of static scratch)");
+                     "glc_trace_static_scratch takes at most 128 scenes and 128 cameras (96 KiB of static scratch)");
   const glc_policy& pol = *policy;
   if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
   if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
@@ -140,7 +140,7 @@ extern "C" glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t 
   const size_t off_begin = off_cams + align256(sizeof(glc_camera) * size_t(n_cameras));
   const size_t job_bytes = off_begin + align256(sizeof(unsigned long long) * size_t(n_cameras + 1));
   if (kQueueBytes + job_bytes > kScratchBytes)
-    return set_error(GLC_ERR_CAPACITY, "job table exceeds the 64 KiB static scratch");
+    return set_error(GLC_ERR_CAPACITY, "job table exceeds the 96 KiB static scratch");
   alignas(256) static thread_local unsigned char stage[kScratchBytes];
   unsigned long long* begin = reinterpret_cast<unsigned long long*>(stage + off_begin);
   unsigned long long acc = 0;

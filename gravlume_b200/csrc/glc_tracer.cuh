@@ -28,6 +28,7 @@
 #endif
 
 #include "glc_dp54.cuh"
+#include "glc_radiation.cuh"
 #include "../../include/glc.h"
 
 namespace glc {
@@ -90,6 +91,8 @@ struct LaneScene {
   double shell_r;     // MIXED binary64 shell radius
   double frequency;
   uint32_t installed; // event bits installed
+  int emission_model;  // surface transport: 0 bolometric, 1 blackbody
+  double intensity_at_six, temperature_at_six, slab_transmittance, slab_emission, slab_bands[3];
 };
 
 GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor) {
@@ -105,6 +108,12 @@ GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor) {
   ls.surf_out = s.surface_outer;
   ls.shell_r = shell_factor * s.photon_shell_radius;
   ls.frequency = s.frequency;
+  ls.emission_model = s.emission_model;
+  ls.intensity_at_six = s.intensity_at_six;
+  ls.temperature_at_six = s.temperature_at_six;
+  ls.slab_transmittance = s.slab_transmittance;
+  ls.slab_emission = s.slab_emission;
+  for (int b = 0; b < 3; ++b) ls.slab_bands[b] = s.slab_bands[b];
   ls.installed = (1u << kEvGuard) | (s.has_horizon ? 1u << kEvHorizon : 0u) | (s.has_surface ? 1u << kEvSurface : 0u) |
                  (s.has_escape ? 1u << kEvEscape : 0u);
   return ls;
@@ -160,6 +169,7 @@ struct RayResult {
   S event_theta;  // fraction of the terminal step at the localized event (read by the adjoint)
   S escape_theta, escape_phi;
   S surface_r, surface_phi, g;
+  double emitted, observed, rgb[3];  // surface transport (valid when observed is finite)
 };
 
 // Dense output of one step as four polynomial coefficient vectors in T (built once from the
@@ -815,6 +825,7 @@ struct Ray {
     res.event_theta = S(NAN);
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
+    res.emitted = res.observed = NAN;
   }
 
   // Terminal observables at the committed event state y (precision S; binary64 in MIXED).
@@ -833,6 +844,7 @@ struct Ray {
     res.event_residual = residual;
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
+    res.emitted = res.observed = NAN;
     if (term == GLC_TERM_ESCAPE) {
       T d[7], rr, vv;
       kn_rhs(kt, ye, E, d, rr, vv);
@@ -854,6 +866,14 @@ struct Ray {
         res.surface_r = rr;
         res.surface_phi = phi;
         res.g = g;
+        // post-hit transport in binary64 (surface.rs:12-72)
+        double em, ob, rgb[3];
+        if (surface_radiance(sc.emission_model, sc.intensity_at_six, sc.temperature_at_six, sc.slab_transmittance,
+                             sc.slab_emission, sc.slab_bands, double(rr), double(g), em, ob, rgb)) {
+          res.emitted = em;
+          res.observed = ob;
+          for (int b = 0; b < 3; ++b) res.rgb[b] = rgb[b];
+        }
       } else {
         flags |= kFlagSurfaceInvalid;
       }

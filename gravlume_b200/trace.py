@@ -60,10 +60,17 @@ def prograde_isco(spin: float, charge: float = 0.0) -> float:
 
 @dataclass
 class EquatorialSurface:
-    """Inclusive radial interval of the Keplerian bolometric emitter (emission.rs:30-41)."""
+    """Inclusive radial interval of the Keplerian emitter (emission.rs:30-41): inverse-cube
+    bolometric intensity I(6 M), or inverse-cube blackbody with temperature T(6 M) when
+    `temperature_at_six` is given; an optional homogeneous scalar slab in front of it (optical depth,
+    integrated bolometric emission, and the slab temperature for the blackbody band split)."""
     inner_radius: float
     outer_radius: float
     intensity_at_six: float = 1.0
+    temperature_at_six: float | None = None
+    slab_optical_depth: float | None = None
+    slab_emission: float = 0.0
+    slab_temperature: float = 0.0
 
 
 @dataclass
@@ -105,6 +112,14 @@ class Observation:
             s.surface_inner = self.surface.inner_radius
             s.surface_outer = self.surface.outer_radius
             s.intensity_at_six = self.surface.intensity_at_six
+            if self.surface.temperature_at_six is not None:
+                s.emission_model = 1
+                s.temperature_at_six = self.surface.temperature_at_six
+            if self.surface.slab_optical_depth is not None:
+                s.has_slab = 1
+                s.slab_optical_depth = self.surface.slab_optical_depth
+                s.slab_emission = self.surface.slab_emission
+                s.slab_temperature = self.surface.slab_temperature
         s.horizon_offset = self.horizon_offset
         return s
 
@@ -163,10 +178,11 @@ class TraceResults:
         self.host = host
         self.buffers = {}
         for name in fields:
+            nb = N.RESULT_BYTES[name]
             if host:
-                t = torch.empty((self.slots, 16), dtype=torch.uint8, pin_memory=True)
+                t = torch.empty((self.slots, nb), dtype=torch.uint8, pin_memory=True)
             else:
-                t = torch.empty((self.slots, 16), dtype=torch.uint8, device=device)
+                t = torch.empty((self.slots, nb), dtype=torch.uint8, device=device)
             t.fill_(0xFF)
             self.buffers[name] = t
 
@@ -204,10 +220,13 @@ class TraceResults:
             "turning": ("turning_radius", "azimuth_advance"), "position_xy": ("x", "y"),
             "position_zr": ("z", "r"),
         }
+        pairs["intensity"] = ("observed_intensity", "emitted_intensity")
         for k, (a, c) in pairs.items():
             if k in b:
                 v = b[k].view(np.float64).reshape(-1, 2)
                 out[a], out[c] = v[:, 0], v[:, 1]
+        if "radiance" in b:
+            out["radiance"] = b["radiance"].view(np.float16).reshape(-1, 4).astype(np.float32)
         return out
 
 

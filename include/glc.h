@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define GLC_ABI_VERSION 1
+#define GLC_ABI_VERSION 2
 
 typedef enum glc_status {
   GLC_OK = 0,
@@ -99,6 +99,14 @@ typedef struct glc_scene_input {
   double surface_inner, surface_outer; /* inclusive radial interval of the surface */
   double intensity_at_six;        /* bolometric I(6 M) of the inverse-cube emitter */
   double horizon_offset;          /* capture at r = r_+ + offset (reference: 0) */
+  /* surface emission and transport (EquatorialEmissionModel, SurfaceTransport: emission.rs,
+   * radiation.rs of gravlume-domain) */
+  int32_t emission_model;         /* 0 inverse-cube bolometric, 1 inverse-cube blackbody */
+  int32_t has_slab;               /* homogeneous scalar slab in front of the surface */
+  double temperature_at_six;      /* K at r = 6 M (blackbody model) */
+  double slab_optical_depth;      /* tau >= 0 */
+  double slab_emission;           /* integrated bolometric emission of the slab >= 0 */
+  double slab_temperature;        /* K: blackbody split of the slab emission (blackbody model) */
 } glc_scene_input;
 
 /* Device-ready packed scene, normalized to M = 1 (the analogue of TraceUniforms, kept in
@@ -119,7 +127,12 @@ typedef struct glc_scene {
   uint32_t width, height;
   int32_t extremality;            /* 0 subextremal, 1 extremal, 2 superextremal */
   int32_t has_horizon, has_escape, has_surface;
-  int32_t reserved[2];
+  int32_t emission_model;         /* 0 bolometric, 1 blackbody */
+  int32_t reserved;
+  double temperature_at_six;      /* K (blackbody) */
+  double slab_transmittance;      /* exp(-tau), 1 without a slab */
+  double slab_emission;           /* integrated bolometric emission, 0 without a slab */
+  double slab_bands[3];           /* its red, green, blue band split (blackbody), else 0 */
 } glc_scene;
 
 /* Step policy: ReferencePolicy fields (policy.rs:26-66) + precision + launch shape. */
@@ -181,10 +194,12 @@ typedef struct glc_camera {
  *   drift_a (max normalized null residual, max relative energy drift)
  *   drift_b (max relative L_z drift, max relative Carter drift)
  *   turning (minimum turning radius or NaN, azimuth advance)
- *   position_xy / position_zr (final x, y) / (final z, final Kerr-Schild radius) */
+ *   position_xy / position_zr (final x, y) / (final z, final Kerr-Schild radius)
+ *   intensity / radiance: post-hit surface transport (see below) */
 typedef struct glc_u32x4 { uint32_t x, y, z, w; } glc_u32x4;
 typedef struct glc_i32x4 { int32_t x, y, z, w; } glc_i32x4;
 typedef struct glc_f64x2 { double x, y; } glc_f64x2;
+typedef struct glc_half4 { uint16_t x, y, z, w; } glc_half4; /* IEEE binary16 bit patterns */
 
 typedef struct glc_results {
   glc_u32x4* code;
@@ -198,6 +213,9 @@ typedef struct glc_results {
   glc_f64x2* turning;
   glc_f64x2* position_xy;
   glc_f64x2* position_zr;
+  glc_f64x2* intensity;           /* (observed bolometric intensity after the slab, emitted) at a surface hit */
+  glc_half4* radiance;            /* RGBA16F, 8 bytes per ray: observed surface radiance (r, g, b, 2)
+                                     at a surface hit, zero elsewhere (surface_transport.wgsl) */
 } glc_results;
 
 typedef struct glc_ctx glc_ctx;
@@ -304,7 +322,7 @@ glc_status glc_tape_destroy(glc_tape* tape);
 /* No counterpart in the reference: its wgpu trace pass always allocates its own target and
  * scratch. For callers that may not allocate device memory (a host whose frame allocator owns the
  * device heap, a plugin confined to buffers its host hands it): the persistent work-queue trace of
- * glc_trace, without a context. Its scratch (queue counter and job table) is a 64 KiB static
+ * glc_trace, without a context. Its scratch (queue counter and job table) is a 96 KiB static
  * device array, so at most 128 scenes and 128 cameras (GLC_ERR_CAPACITY beyond). Runs on the
  * current device; the first call on a device looks up the array's address, so make it before any
  * stream capture. All calls share the array: calls that overlap on the GPU race. Scenes, cameras

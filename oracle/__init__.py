@@ -294,3 +294,33 @@ def hamiltonian_rhs(mass, spin, charge, chart, state):
 
 def default_threads() -> int:
     return max(1, int(os.environ.get("GRO_THREADS", "0")) or hardware_threads())
+
+
+def planck_integral(lo, hi):
+    """int_lo^hi x^3 / (e^x - 1) dx by the reference's quadrature (radiation.rs:113-161)."""
+    f = lib().gro_planck_integral
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double, ctypes.c_double]
+    return f(lo, hi)
+
+
+def blackbody_bands(intensity, temperature):
+    """Red, green, blue boxcar band intensities of a bolometric intensity at a temperature
+    (radiation.rs:13-31); None when not representable."""
+    f = lib().gro_blackbody_bands
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    out = np.zeros(3)
+    return out if f(intensity, temperature, out.ctypes.data) else None
+
+
+def surface_radiance(model, intensity_at_six, temperature_at_six, r, g, slab=None):
+    """(emitted, observed bolometric, r, g, b) of a surface hit at radius r with frequency ratio g
+    (surface.rs:12-72); slab = (optical depth, integrated emission, temperature) or None."""
+    f = lib().gro_surface_radiance
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    tau, s, ts = slab if slab is not None else (0.0, 0.0, 0.0)
+    out = np.zeros(5)
+    ok = f(int(model), intensity_at_six, temperature_at_six, 1 if slab is not None else 0, tau, s, ts, r, g,
+           out.ctypes.data)
+    return out if ok else None

@@ -11,6 +11,7 @@
 #include <thread>
 #include <vector>
 
+#include "oracle_radiation.hpp"
 #include "oracle_tracer.hpp"
 
 using namespace gro;
@@ -312,6 +313,18 @@ int gro_hamiltonian_rhs(double m, double a, double q, int chart, const double* s
   Spacetime sp;
   if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
   return int(sp.hamiltonian_rhs(state, out8));
+}
+
+// Surface radiation model (radiation.rs, surface.rs): Planck integral, band split, radiance.
+double gro_planck_integral(double lo, double hi) { return integrate_planck(lo, hi); }
+
+int gro_blackbody_bands(double intensity, double temperature, double* out3) {
+  return blackbody_bands(intensity, temperature, out3) ? 1 : 0;
+}
+
+int gro_surface_radiance(int model, double i6, double t6, int slab, double tau, double s, double tslab, double r,
+                         double g, double* out5) {
+  return surface_radiance(model, i6, t6, slab != 0, tau, s, tslab, r, g, out5) ? 1 : 0;
 }
 
 }  // extern "C"

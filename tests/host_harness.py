@@ -71,3 +71,19 @@ def trace_perturbed(scene, policy, states, direction, da=0.0, dq2=0.0):
                                     direction, da, dq2, out.ctypes.data)
     assert rc == 0
     return out
+
+
+def blackbody_bands(intensity, temperature):
+    f = lib().host_blackbody_bands
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    out = np.zeros(3)
+    return out if f(intensity, temperature, out.ctypes.data) else None
+
+
+def surface_radiance(model, i6, t6, r, g, slab=None):
+    f = lib().host_surface_radiance
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    tau, s, ts = slab if slab is not None else (0.0, 0.0, 0.0)
+    out = np.zeros(5)
+    return out if f(int(model), i6, t6, 1 if slab is not None else 0, tau, s, ts, r, g, out.ctypes.data) else None

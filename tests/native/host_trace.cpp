@@ -160,3 +160,21 @@ extern "C" int host_trace_perturbed(const glc_scene* sc, const glc_policy* pol, 
   }
   return -1;
 }
+
+// The device's surface transport (glc_radiation.cuh) for the CPU checks.
+extern "C" int host_blackbody_bands(double intensity, double temperature, double* out3) {
+  return blackbody_bands(intensity, temperature, out3) ? 1 : 0;
+}
+
+extern "C" int host_surface_radiance(int model, double i6, double t6, int slab, double tau, double s, double tslab,
+                                     double r, double g, double* out5) {
+  double bands[3] = {0.0, 0.0, 0.0};
+  if (slab && model == 1 && s > 0.0 && !blackbody_bands(s, tslab, bands)) return 0;
+  const double trans = slab ? std::exp(-tau) : 1.0;
+  double em, ob, rgb[3];
+  if (!surface_radiance(model, i6, t6, trans, slab ? s : 0.0, bands, r, g, em, ob, rgb)) return 0;
+  out5[0] = em;
+  out5[1] = ob;
+  for (int b = 0; b < 3; ++b) out5[2 + b] = rgb[b];
+  return 1;
+}

@@ -31,7 +31,9 @@ def test_library_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), name
         assert name in N.SIGNATURES, f"{name} has no ctypes signature"
-    assert lib.glc_abi_version() == 1
+    header = (ROOT / "include" / "glc.h").read_text()
+    assert f"#define GLC_ABI_VERSION {N.ABI_VERSION}" in header
+    assert lib.glc_abi_version() == N.ABI_VERSION
     assert lib.glc_status_string(0) == b"ok"
 
 
