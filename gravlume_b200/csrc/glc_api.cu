@@ -13,6 +13,7 @@
 #include "glc_internal.h"
 #include "glc_certificate.cuh"
 #include "glc_escape_map.cuh"
+#include "glc_shadow.cuh"
 
 using namespace glc;
 
@@ -454,6 +455,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_queue) cudaFree(ctx->d_queue);
   if (ctx->d_cert) cudaFree(ctx->d_cert);
   if (ctx->d_emap) cudaFree(ctx->d_emap);
+  if (ctx->d_shadow) cudaFree(ctx->d_shadow);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
@@ -521,6 +523,54 @@ glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, co
   }
   return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue, ctx->d_cert, tiles,
                 ctx->d_emap, nodes);
+}
+
+glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
+                                   const glc_camera* cameras, int32_t n_cameras, const glc_results* primary,
+                                   float* coverage, void* stream) {
+  if (!ctx || !primary || !primary->code || !coverage) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(ctx->device);
+  JobLayout L;
+  glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
+  if (s != GLC_OK) return s;
+  s = ensure_job_capacity(ctx, L.bytes);
+  if (s != GLC_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  fill_staging(ctx->h_stage, L, scenes, n_scenes, cameras, n_cameras);
+  GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, st));
+  GLC_CUDA(cudaEventRecord(ctx->stage_free, st));
+  ctx->stage_pending = true;
+  const JobView job = job_view(ctx->d_job, L, n_cameras);
+  // edge-list capacity: every pixel of every image camera, plus the counter word
+  unsigned long long pixels = 0;
+  for (int i = 0; i < n_cameras; ++i)
+    if (cameras[i].kind != GLC_CAMERA_RAYLIST) pixels += (unsigned long long)cameras[i].width * cameras[i].height;
+  if (pixels == 0) return GLC_OK;
+  if (pixels > 0xffffffffull) return set_error(GLC_ERR_CAPACITY, "too many image pixels for one refinement");
+  s = ensure_cert_capacity(&ctx->d_shadow, &ctx->d_shadow_words, 2 * pixels + 2);
+  if (s != GLC_OK) return s;
+  unsigned int* count = ctx->d_shadow;
+  unsigned long long* list = reinterpret_cast<unsigned long long*>(ctx->d_shadow + 2);
+  GLC_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned int), st));
+  const uint4* code = reinterpret_cast<const uint4*>(primary->code);
+  for (int i = 0; i < n_cameras; ++i) {
+    if (cameras[i].kind == GLC_CAMERA_RAYLIST) continue;
+    const unsigned long long np = (unsigned long long)cameras[i].width * cameras[i].height;
+    shadow_classify_kernel<<<unsigned((np + 255) / 256), 256, 0, st>>>(job, i, code, coverage, list, count,
+                                                                     unsigned(pixels));
+    GLC_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+  }
+  const glc_policy& pol = ctx->policy;
+  const unsigned grid = unsigned(ctx->sm_count) * 8u;
+  switch (pol.precision) {
+    case GLC_FP32: shadow_refine_kernel<kFP32><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
+    case GLC_MIXED: shadow_refine_kernel<kMIXED><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
+    default: shadow_refine_kernel<kFP64><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
+  }
+  GLC_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches += 1;
+  return GLC_OK;
 }
 
 glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,

@@ -388,6 +388,18 @@ class TracePipeline:
                                   self._stream(stream)), "glc_trace")
         return results
 
+    def refine_shadow_edges(self, scenes, cameras, primary: TraceResults, stream=None):
+        """Coverage per result slot after glc_trace of the same job into `primary`: 1 escape, 0 capture,
+        the escaping fraction of four subpixel samples on capture/escape edges, -1 elsewhere."""
+        torch = _torch()
+        cov = torch.full((primary.slots,), -1.0, dtype=torch.float32, device=torch.device("cuda", self.device))
+        sa, ca = self._arrays(scenes, cameras)
+        rs = primary.struct()
+        N.check(N.lib().glc_refine_shadow_edges(self._h, sa, len(scenes), ca, len(cameras), ctypes.byref(rs),
+                                                ctypes.c_void_p(cov.data_ptr()), self._stream(stream)),
+                "glc_refine_shadow_edges")
+        return cov
+
     def forward_ckpt(self, observation: Observation, radius: float, polar: float, azimuth: float = 0.0,
                      K: int = 64, states=None, direction: float = -1.0, stream=None):
         """Forward trace with checkpoints every K accepted steps (glc_forward_ckpt). The observer sits

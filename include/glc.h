@@ -269,6 +269,17 @@ glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, co
 glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
                           int32_t n_cameras, const glc_results* host_out);
 
+/* Shadow-edge coverage refinement (shadow_coverage.wgsl:63-136, classify_shadow_edges and
+ * refine_shadow_edges): after a glc_trace of the same job into `primary` (its code array is read),
+ * coverage[slot] is 1 for escape and 0 for capture pixels of image cameras, -1 for any other
+ * class; capture/escape pixels with a 4-neighbour of the other class are re-traced with four
+ * rotated-grid subpixel samples (0.375, 0.125), (0.875, 0.375), (0.625, 0.875), (0.125, 0.625) and
+ * get the fraction of escaping samples, unless a sample ends another way. coverage is a device
+ * float array as long as the results. Stream-ordered, no host synchronization. */
+glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
+                                   const glc_camera* cameras, int32_t n_cameras, const glc_results* primary,
+                                   float* coverage, void* stream);
+
 /* ---- CUDA graphs (per-frame replay of the job-table copy, queue reset and trace launch) ---- */
 glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
                              int32_t n_cameras, const glc_results* out, void* stream, glc_graph** graph);
