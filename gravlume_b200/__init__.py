@@ -9,6 +9,6 @@ host binding over that C ABI.
 from ._native import GlcError, lib  # noqa: F401
 from .build import LIB_PATH, build  # noqa: F401
 from .trace import (  # noqa: F401
-    EquatorialSurface, Graph, KerrSchildChart, Observation, Precision, ReferencePolicy, Termination,
-    Tape, TracePipeline, TraceResults, image_camera, oblate_to_cartesian, prograde_isco, raylist_camera,
+    EquatorialSurface, FootprintStatus, Graph, KerrSchildChart, Observation, Precision, ReferencePolicy, Termination,
+    Tape, TracePipeline, TraceResults, footprint_fields, image_camera, oblate_to_cartesian, prograde_isco, raylist_camera,
 )

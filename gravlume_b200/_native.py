@@ -135,6 +135,8 @@ SIGNATURES = {
                                ctypes.POINTER(Results), c_void_p, c_int32, ctypes.POINTER(Policy)]),
     "glc_refine_shadow_edges": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_int32, ctypes.POINTER(Results),
                                           c_void_p, c_void_p]),
+    "glc_surface_footprint": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32,
+                                        ctypes.POINTER(Results), c_void_p, c_void_p]),
     "glc_forward_ckpt": (c_int32, [c_void_p, ctypes.POINTER(AdjointScene), ctypes.POINTER(Camera), c_int32,
                                    ctypes.POINTER(Results), c_void_p, ctypes.POINTER(c_void_p)]),
     "glc_backward": (c_int32, [c_void_p, c_void_p, ctypes.POINTER(Grads), c_void_p]),

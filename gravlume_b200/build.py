@@ -18,7 +18,7 @@ LIB_DIR = PKG / "_lib"
 LIB_PATH = LIB_DIR / "libglc.so"
 
 SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_adjoint.cu", "glc_scene.cpp", "glc_flops.cpp"]
-HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh", "glc_escape_map.cuh", "glc_shadow.cuh",
+HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh", "glc_escape_map.cuh", "glc_shadow.cuh", "glc_footprint.cuh",
            "glc_dual.cuh", "glc_adjoint.cuh", "glc_radiation.cuh", "glc_internal.h", "glc_context.h"]
 
 NVCC_FLAGS = [

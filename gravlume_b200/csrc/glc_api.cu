@@ -14,6 +14,7 @@
 #include "glc_certificate.cuh"
 #include "glc_escape_map.cuh"
 #include "glc_shadow.cuh"
+#include "glc_footprint.cuh"
 
 using namespace glc;
 
@@ -456,6 +457,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_cert) cudaFree(ctx->d_cert);
   if (ctx->d_emap) cudaFree(ctx->d_emap);
   if (ctx->d_shadow) cudaFree(ctx->d_shadow);
+  if (ctx->d_footprint) cudaFree(ctx->d_footprint);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
@@ -567,6 +569,74 @@ glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_
     case GLC_FP32: shadow_refine_kernel<kFP32><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
     case GLC_MIXED: shadow_refine_kernel<kMIXED><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
     default: shadow_refine_kernel<kFP64><<<grid, 128, 0, st>>>(job, pol, list, count, unsigned(pixels), coverage); break;
+  }
+  GLC_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches += 1;
+  return GLC_OK;
+}
+
+glc_status glc_surface_footprint(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                                 int32_t n_cameras, int32_t method, const glc_results* primary, glc_footprint* out,
+                                 void* stream) {
+  if (!ctx || !primary || !primary->code || !out || !cameras) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (method != GLC_FOOTPRINT_QUARTER_PIXEL && method != GLC_FOOTPRINT_TANGENT)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown footprint method");
+  if (method == GLC_FOOTPRINT_QUARTER_PIXEL && (!primary->branch || !primary->surface))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "the quarter-pixel footprint reads the primary branch and surface arrays");
+  for (int i = 0; i < n_cameras; ++i) {
+    if (cameras[i].kind == GLC_CAMERA_RAYLIST)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "surface footprints are defined for image cameras only");
+    const double sx = cameras[i].subpixel_x, sy = cameras[i].subpixel_y;
+    // footprint.rs:82-86: the centered quarter-pixel stencil must stay inside the pixel
+    if (method == GLC_FOOTPRINT_QUARTER_PIXEL && !(sx >= 0.25 && sx <= 0.75 && sy >= 0.25 && sy <= 0.75))
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "surface footprint requires subpixel coordinates in [0.25, 0.75]");
+  }
+  DeviceGuard g(ctx->device);
+  JobLayout L;
+  glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
+  if (s != GLC_OK) return s;
+  s = ensure_job_capacity(ctx, L.bytes);
+  if (s != GLC_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  fill_staging(ctx->h_stage, L, scenes, n_scenes, cameras, n_cameras);
+  GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, st));
+  GLC_CUDA(cudaEventRecord(ctx->stage_free, st));
+  ctx->stage_pending = true;
+  const JobView job = job_view(ctx->d_job, L, n_cameras);
+  unsigned long long pixels = 0;
+  for (int i = 0; i < n_cameras; ++i) pixels += (unsigned long long)cameras[i].width * cameras[i].height;
+  if (pixels == 0) return GLC_OK;
+  if (pixels > 0xffffffffull) return set_error(GLC_ERR_CAPACITY, "too many image pixels for one footprint call");
+  s = ensure_cert_capacity(&ctx->d_footprint, &ctx->d_footprint_words, 2 * pixels + 2);
+  if (s != GLC_OK) return s;
+  unsigned int* count = ctx->d_footprint;
+  unsigned long long* list = reinterpret_cast<unsigned long long*>(ctx->d_footprint + 2);
+  GLC_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned int), st));
+  const uint4* code = reinterpret_cast<const uint4*>(primary->code);
+  for (int i = 0; i < n_cameras; ++i) {
+    const unsigned long long np = (unsigned long long)cameras[i].width * cameras[i].height;
+    footprint_classify_kernel<<<unsigned((np + 255) / 256), 256, 0, st>>>(job, i, code, out, list, count,
+                                                                        unsigned(pixels));
+    GLC_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+  }
+  const glc_policy& pol = ctx->policy;
+  const unsigned grid = unsigned(ctx->sm_count) * 8u;
+  const unsigned cap = unsigned(pixels);
+  if (method == GLC_FOOTPRINT_QUARTER_PIXEL) {
+    const int4* branch = reinterpret_cast<const int4*>(primary->branch);
+    const double2* surface = reinterpret_cast<const double2*>(primary->surface);
+    switch (pol.precision) {
+      case GLC_FP32: footprint_quarter_kernel<kFP32><<<grid, 128, 0, st>>>(job, pol, list, count, cap, code, branch, surface, out); break;
+      case GLC_MIXED: footprint_quarter_kernel<kMIXED><<<grid, 128, 0, st>>>(job, pol, list, count, cap, code, branch, surface, out); break;
+      default: footprint_quarter_kernel<kFP64><<<grid, 128, 0, st>>>(job, pol, list, count, cap, code, branch, surface, out); break;
+    }
+  } else {
+    switch (pol.precision) {
+      case GLC_FP32: footprint_tangent_kernel<kFP32><<<grid, 128, 0, st>>>(job, pol, list, count, cap, out); break;
+      case GLC_MIXED: footprint_tangent_kernel<kMIXED><<<grid, 128, 0, st>>>(job, pol, list, count, cap, out); break;
+      default: footprint_tangent_kernel<kFP64><<<grid, 128, 0, st>>>(job, pol, list, count, cap, out); break;
+    }
   }
   GLC_CUDA(cudaGetLastError());
   ctx->stats.kernel_launches += 1;

@@ -25,6 +25,8 @@ struct glc_ctx {
   size_t d_emap_words = 0;
   uint32_t* d_shadow = nullptr;        // shadow-edge list: counter word pair, then u64 entries (grow-only)
   size_t d_shadow_words = 0;
+  uint32_t* d_footprint = nullptr;     // surface-footprint pixel list: counter word pair, then u64 entries
+  size_t d_footprint_words = 0;
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
   size_t d_host_ws_bytes = 0;
   glc_launch_stats stats{};

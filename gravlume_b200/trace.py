@@ -44,6 +44,29 @@ class Termination(IntEnum):
     REJECT_EXHAUSTION = 8
 
 
+class FootprintStatus(IntEnum):
+    """Per-pixel outcome of glc_surface_footprint (footprint.rs:12-16, 258-268)."""
+    NO_SURFACE = 0
+    RESOLVED = 1
+    DISCONTINUITY = 2
+    NON_FINITE = 3
+
+
+FOOTPRINT_QUARTER_PIXEL = 0
+FOOTPRINT_TANGENT = 1
+
+
+def footprint_fields(fp) -> dict:
+    """Split the (slots, 8) footprint array of TracePipeline.surface_footprint (a tensor or a numpy
+    array) into numpy fields: jacobian (slots, 2, 2; rows radius and local arc, columns screen x and
+    y), singular_values (slots, 2), determinant, status and parity."""
+    a = fp.cpu().numpy() if hasattr(fp, "cpu") else np.asarray(fp)
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    tail = a[:, 7].copy().view(np.int32).reshape(-1, 2)
+    return {"jacobian": a[:, :4].reshape(-1, 2, 2), "singular_values": a[:, 4:6], "determinant": a[:, 6],
+            "status": tail[:, 0].copy(), "parity": tail[:, 1].copy()}
+
+
 def oblate_to_cartesian(spin: float, chart: int, radius: float, polar: float, azimuth: float):
     """KerrNewmanSpacetime::oblate_to_cartesian (crates/gravlume-domain/src/spacetime.rs:245-254)."""
     st, ct = math.sin(polar), math.cos(polar)
@@ -399,6 +422,23 @@ class TracePipeline:
                                                 ctypes.c_void_p(cov.data_ptr()), self._stream(stream)),
                 "glc_refine_shadow_edges")
         return cov
+
+    def surface_footprint(self, scenes, cameras, primary: TraceResults, method: str = "quarter_pixel",
+                          stream=None):
+        """Surface footprints (glc_surface_footprint) after glc_trace of the same job into `primary`:
+        a (slots, 8) float64 device tensor of J (dr/dx, dr/dy, darc/dx, darc/dy; M per pixel), major
+        and minor singular values, determinant, and the status and parity as int32 pairs in the
+        last column's bytes; use `footprint_fields` to split it. method "quarter_pixel" is the
+        reference's estimate, "tangent" the forward-mode derivative of the computed trace."""
+        torch = _torch()
+        m = {"quarter_pixel": FOOTPRINT_QUARTER_PIXEL, "tangent": FOOTPRINT_TANGENT}[method]
+        out = torch.empty((primary.slots, 8), dtype=torch.float64, device=torch.device("cuda", self.device))
+        sa, ca = self._arrays(scenes, cameras)
+        rs = primary.struct()
+        N.check(N.lib().glc_surface_footprint(self._h, sa, len(scenes), ca, len(cameras), m, ctypes.byref(rs),
+                                              ctypes.c_void_p(out.data_ptr()), self._stream(stream)),
+                "glc_surface_footprint")
+        return out
 
     def forward_ckpt(self, observation: Observation, radius: float, polar: float, azimuth: float = 0.0,
                      K: int = 64, states=None, direction: float = -1.0, stream=None):

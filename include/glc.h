@@ -280,6 +280,41 @@ glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_
                                    const glc_camera* cameras, int32_t n_cameras, const glc_results* primary,
                                    float* coverage, void* stream);
 
+/* ---- surface footprint (footprint.rs:74-235) --------------------------------------------- */
+/* Local source Jacobian of an image pixel that ends on the surface: rows (source radius, local
+ * azimuthal arc r_c * dphi), columns (screen x, screen y), in M per image pixel (footprint.rs:30-32);
+ * its singular values (major, minor; minor = |det| / major) and parity (+1, -1, 0 within
+ * 64 eps |J|_F^2 of a zero determinant). 64 bytes. */
+typedef struct glc_footprint {
+  double jacobian[4];        /* dr/dx, dr/dy, darc/dx, darc/dy */
+  double singular_values[2]; /* major, minor */
+  double determinant;
+  int32_t status;            /* GLC_FOOTPRINT_* */
+  int32_t parity;
+} glc_footprint;
+
+#define GLC_FOOTPRINT_NO_SURFACE 0    /* center is not an unambiguous observed surface hit (CenterSurfaceUnavailable) */
+#define GLC_FOOTPRINT_RESOLVED 1
+#define GLC_FOOTPRINT_DISCONTINUITY 2 /* a neighbour left the surface or the center's branch key */
+#define GLC_FOOTPRINT_NON_FINITE 3    /* NonFiniteJacobian */
+
+/* QUARTER_PIXEL: the reference's estimate (surface_footprint_v1): the four neighbours a quarter
+ * pixel left, right, up and down are traced, and the Jacobian is their central difference over
+ * the half-pixel span; needs camera subpixels in [0.25, 0.75]. TANGENT: the exact derivative of
+ * the computed trace in forward mode (two tangent channels through the ray set-up, every accepted
+ * step at its frozen size and the terminal event time), one re-trace per pixel; it does not test
+ * the neighbourhood and never reports DISCONTINUITY. */
+#define GLC_FOOTPRINT_QUARTER_PIXEL 0
+#define GLC_FOOTPRINT_TANGENT 1
+
+/* After a glc_trace of the same job into `primary` (code, branch and surface arrays are read),
+ * out[slot] (a device array as long as the results) receives the footprint of every pixel of the
+ * image cameras; entries that are not RESOLVED hold NaN. Ray-list cameras are rejected.
+ * Stream-ordered, no host synchronization. */
+glc_status glc_surface_footprint(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
+                                 int32_t n_cameras, int32_t method, const glc_results* primary, glc_footprint* out,
+                                 void* stream);
+
 /* ---- CUDA graphs (per-frame replay of the job-table copy, queue reset and trace launch) ---- */
 glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
                              int32_t n_cameras, const glc_results* out, void* stream, glc_graph** graph);

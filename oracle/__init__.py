@@ -324,3 +324,36 @@ def surface_radiance(model, intensity_at_six, temperature_at_six, r, g, slab=Non
     ok = f(int(model), intensity_at_six, temperature_at_six, 1 if slab is not None else 0, tau, s, ts, r, g,
            out.ctypes.data)
     return out if ok else None
+
+
+def surface_footprint(sc: Scene, policy, ev, px, py, sx=0.5, sy=0.5, threads=1):
+    """Quarter-pixel surface footprints (footprint.rs:74-150) of pixel samples: (n, 8) rows of
+    J (dr/dx, dr/dy, darc/dx, darc/dy; M per pixel), major, minor, determinant, parity (NaN unless
+    resolved), and the status per sample (0 no surface, 1 resolved, 2 discontinuity, 3 non-finite)."""
+    px = _c(px, np.uint32)
+    n = px.size
+    py = _c(py, np.uint32)
+    sx = _c(np.broadcast_to(sx, (n,)), np.float64)
+    sy = _c(np.broadcast_to(sy, (n,)), np.float64)
+    out = np.full((n, 8), np.nan)
+    status = np.zeros(n, np.int32)
+    f = lib().gro_surface_footprint
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    rc = f(ctypes.byref(sc), ctypes.byref(policy), ctypes.byref(ev), n, px.ctypes.data, py.ctypes.data,
+           sx.ctypes.data, sy.ctypes.data, threads, out.ctypes.data, status.ctypes.data)
+    if rc == -5:
+        raise ValueError("surface footprint requires subpixel coordinates in [0.25, 0.75]")
+    if rc != 0:
+        raise ValueError(f"trace configuration rejected ({rc})")
+    return out, status
+
+
+def footprint_metrics(jacobian):
+    """(determinant, squared norm, major, minor) of a 2x2 Jacobian (footprint.rs:203-235), or None
+    when it is not finite."""
+    f = lib().gro_footprint_metrics
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    j = _c(np.asarray(jacobian, dtype=np.float64).reshape(4), np.float64)
+    out = np.zeros(4)
+    return out if f(j.ctypes.data, out.ctypes.data) else None

@@ -11,6 +11,7 @@
 #include <thread>
 #include <vector>
 
+#include "oracle_footprint.hpp"
 #include "oracle_radiation.hpp"
 #include "oracle_tracer.hpp"
 
@@ -325,6 +326,52 @@ int gro_blackbody_bands(double intensity, double temperature, double* out3) {
 int gro_surface_radiance(int model, double i6, double t6, int slab, double tau, double s, double tslab, double r,
                          double g, double* out5) {
   return surface_radiance(model, i6, t6, slab != 0, tau, s, tslab, r, g, out5) ? 1 : 0;
+}
+
+// Surface footprint (footprint.rs:74-150) of n pixel samples: the center and its four quarter-pixel
+// neighbours traced through the observation. out8 per sample as gro::surface_footprint; status =
+// FootprintStatus, or -100 - InitialRayError for a sample whose rays cannot be set up.
+int gro_surface_footprint(const gro_scene* s, const gro_policy* pol, const gro_events* ev, int64_t n,
+                          const uint32_t* px, const uint32_t* py, const double* sx, const double* sy, int threads,
+                          double* out8, int32_t* status) {
+  Spacetime sp;
+  StationaryObserver obs;
+  PerspectiveView view;
+  const int rc = build_scene(*s, sp, obs, view);
+  if (rc != 0) return rc;
+  if (bits_of(sp.mass_m) != bits_of(1.0)) return -2;
+  Tracer tr{sp, to_policy(*pol), to_events(*ev)};
+  if (tr.events.has_surface && tr.events.has_escape && tr.events.surface_outer >= tr.events.escape_radius)
+    return -4;
+  for (int64_t i = 0; i < n; ++i)
+    if (!(sx[i] >= 0.25 && sx[i] <= 0.75 && sy[i] >= 0.25 && sy[i] <= 0.75)) return -5;  // footprint.rs:82-86
+  parallel_for(n, threads, [&](int64_t i) {
+    const double off[5][2] = {{0.0, 0.0}, {-0.25, 0.0}, {0.25, 0.0}, {0.0, -0.25}, {0.0, 0.25}};
+    Outcome o[5];
+    for (int k = 0; k < 5; ++k) {
+      InitialRay ray;
+      const InitialRayError e = initial_ray(obs, view, px[i], py[i], sx[i] + off[k][0], sy[i] + off[k][1], ray);
+      if (e != InitialRayError::None) {
+        status[i] = -100 - int(e);
+        for (int j = 0; j < 8; ++j) out8[8 * i + j] = NAN;
+        return;
+      }
+      o[k] = trace_observation(tr, ray, ev->intensity_at_six);
+    }
+    status[i] = surface_footprint(o, out8 + 8 * i);
+  });
+  return 0;
+}
+
+// footprint.rs:203-235 on one Jacobian: out4 = determinant, squared norm, major, minor.
+int gro_footprint_metrics(const double* J, double* out4) {
+  FootprintMetrics m;
+  if (!footprint_metrics(J, m)) return 0;
+  out4[0] = m.determinant;
+  out4[1] = m.squared_norm;
+  out4[2] = m.major;
+  out4[3] = m.minor;
+  return 1;
 }
 
 }  // extern "C"
