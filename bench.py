@@ -393,6 +393,7 @@ def run_gpu(args) -> None:
     if args.batch:
         line["batch"] = batch_study(G, local)
         line["sky"] = sky_study(G, local)
+    if args.footprint:
         line["footprint"] = footprint_study(G, local, args.cpu_sample > 0)
     print(json.dumps(line), flush=True)
     if dist:
@@ -714,6 +715,8 @@ def main() -> None:
     ap.add_argument("--adjoint-side", type=int, default=1024)
     ap.add_argument("--no-sweep", dest="sweep", action="store_false",
                     help="skip the tolerance sweep of the precision study")
+    ap.add_argument("--no-footprint", dest="footprint", action="store_false",
+                    help="skip the surface-footprint study")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-scene batch study (persistent launch, graph, autotuner)")
     ap.add_argument("--adjoint-k", type=int, nargs="+", default=[16, 64, 256])

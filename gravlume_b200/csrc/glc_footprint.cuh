@@ -180,11 +180,14 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) footprint_qua
   }
 }
 
-// Slopes K_i of the step from y0 with size h (frozen), in dual arithmetic.
-__device__ __noinline__ void dual_stages(const KN<double>& k, const D2 y0[6], const D2& E, double h, D2 K[7][6]) {
+// Slopes K_i, i < kStages, of the step from y0 with size h (frozen), in dual arithmetic.
+template <int kStages>
+__device__ __forceinline__ void dual_stages(const KN<double>& k, const D2 y0[6], const D2& E, double h,
+                                            D2 K[kStages][6]) {
   const KN<D2> kt{D2(k.a), D2(k.a2), D2(k.s), D2(k.sa), D2(k.q2)};
-  for (int i = 0; i < 7; ++i) {
+  for (int i = 0; i < kStages; ++i) {
     D2 Y[6];
+#pragma unroll
     for (int c = 0; c < 6; ++c) {
       D2 s(0.0);
       for (int j = 0; j < i; ++j) s += dp_coef(i, j) * K[j][c];
@@ -192,19 +195,23 @@ __device__ __noinline__ void dual_stages(const KN<double>& k, const D2 y0[6], co
     }
     D2 d[7], r, vr;
     kn_rhs(kt, Y, E, d, r, vr);
+#pragma unroll
     for (int c = 0; c < 6; ++c) K[i][c] = d[c];
   }
 }
 
-// Tangent of an accepted step: y <- y + h sum_i b_i K_i with the stages in dual arithmetic.
+// Tangent of an accepted step: y <- y + h sum_i b_i K_i with the stages in dual arithmetic (the
+// seventh stage, the slope at the end point, has weight 0).
 __device__ __noinline__ void step_tangent(const KN<double>& k, D2 y[6], const D2& E, double h) {
-  D2 K[7][6];
-  dual_stages(k, y, E, h, K);
+  D2 K[6][6];
+  dual_stages<6>(k, y, E, h, K);
   double w[7];
   step_weights(w);
+#pragma unroll
   for (int c = 0; c < 6; ++c) {
     D2 s(0.0);
-    for (int i = 0; i < 7; ++i) s += w[i] * K[i][c];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s += w[i] * K[i][c];
     y[c] = y[c] + h * s;
   }
 }
@@ -213,7 +220,7 @@ __device__ __noinline__ void step_tangent(const KN<double>& k, D2 y[6], const D2
 // event time moving so that z stays 0 (d theta = -dz / zdot).
 __device__ __noinline__ void hit_tangent(const KN<double>& k, D2 y[6], const D2& E, double h, double theta) {
   D2 K[7][6];
-  dual_stages(k, y, E, h, K);
+  dual_stages<7>(k, y, E, h, K);
   double w[7], dw[7];
   dense_weights_at(theta, w, dw);
   D2 ys[6];
