@@ -139,6 +139,8 @@ SIGNATURES = {
                                         ctypes.POINTER(Results), c_void_p, c_void_p]),
     "glc_forward_ckpt": (c_int32, [c_void_p, ctypes.POINTER(AdjointScene), ctypes.POINTER(Camera), c_int32,
                                    ctypes.POINTER(Results), c_void_p, ctypes.POINTER(c_void_p)]),
+    "glc_forward_ckpt_into": (c_int32, [c_void_p, ctypes.POINTER(AdjointScene), ctypes.POINTER(Camera), c_int32,
+                                        ctypes.POINTER(Results), c_void_p, c_void_p]),
     "glc_backward": (c_int32, [c_void_p, c_void_p, ctypes.POINTER(Grads), c_void_p]),
     "glc_tape_info": (c_int32, [c_void_p, ctypes.POINTER(c_uint64), ctypes.POINTER(c_uint32),
                                 ctypes.POINTER(c_uint64)]),

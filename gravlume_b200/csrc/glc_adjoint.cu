@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
   double rdir[3];
   ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir);
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
-  const KN<D9> kd = kn_dual(ls.kn);
+  const KN<D4> kd = kn_dual_vjp(ls.kn);
   double wobs[kObs];
   bool any = false;
   for (int k = 0; k < kObs; ++k) {
@@ -250,8 +250,9 @@ struct glc_tape {
   unsigned char* d_job = nullptr;
   size_t off_cams = 0, off_begin = 0, off_cert = 0;
   uint4* d_ckpt = nullptr;
-  size_t ckpt_bytes = 0;
+  size_t ckpt_bytes = 0, ckpt_alloc = 0;
   uint4* d_meta = nullptr;
+  unsigned long long meta_alloc = 0;
   double* d_dconst = nullptr;
   double* d_scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -306,12 +307,17 @@ glc_status forward(glc_tape* t, const glc_results& out, cudaStream_t st) {
   return t->pol.precision == GLC_MIXED ? run_forward<kMIXED>(t, out, st) : run_forward<kFP64>(t, out, st);
 }
 
+// Checkpoint slots for every ray; the allocation only grows (a reused tape keeps its memory).
 glc_status size_checkpoints(glc_tape* t, uint32_t cap) {
-  if (t->d_ckpt) cudaFree(t->d_ckpt);
-  t->d_ckpt = nullptr;
   t->cap = cap;
   t->ckpt_bytes = size_t(cap) * t->words * 16 * t->n;
-  return cuda_status(cudaMalloc(&t->d_ckpt, t->ckpt_bytes));
+  if (t->ckpt_bytes <= t->ckpt_alloc) return GLC_OK;
+  if (t->d_ckpt) cudaFree(t->d_ckpt);
+  t->d_ckpt = nullptr;
+  t->ckpt_alloc = 0;
+  const glc_status s = cuda_status(cudaMalloc(&t->d_ckpt, t->ckpt_bytes));
+  if (s == GLC_OK) t->ckpt_alloc = t->ckpt_bytes;
+  return s;
 }
 
 struct DeviceScope {
@@ -325,14 +331,10 @@ struct DeviceScope {
   }
 };
 
-}  // namespace
-
-extern "C" {
-
-glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc_camera* camera, int32_t K,
-                            const glc_results* out, void* stream, glc_tape** tape) {
-  if (!ctx || !as || !camera || !out || !tape) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
-  *tape = nullptr;
+// Validates the request and runs the forward pass into t (a new tape, or one being reused: its
+// buffers are kept and grown only where this request needs more).
+glc_status fill_tape(glc_tape* t, glc_ctx* ctx, const glc_adjoint_scene* as, const glc_camera* camera, int32_t K,
+                     const glc_results* out, void* stream) {
   if (K < 1) return set_error(GLC_ERR_INVALID_ARGUMENT, "checkpoint interval K must be at least 1");
   const glc_policy pol = ctx->policy;
   if (pol.precision != GLC_MIXED && pol.precision != GLC_FP64)
@@ -386,8 +388,6 @@ glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc
     }
   }
 
-  DeviceScope scope(ctx->device);
-  glc_tape* t = new glc_tape();
   t->ctx = ctx;
   t->pol = pol;
   t->cam = *camera;
@@ -400,10 +400,6 @@ glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc
   t->off_begin = t->off_cams + align256(sizeof(glc_camera));
   t->off_cert = t->off_begin + 256;
   const size_t job_bytes = t->off_cert + 256;
-  auto fail = [&](glc_status st) {
-    free_tape(t);
-    return st;
-  };
   alignas(16) static thread_local unsigned char host_job[4096];
   std::memset(host_job, 0, sizeof(host_job));
   std::memcpy(host_job, &scene, sizeof(glc_scene));
@@ -412,30 +408,64 @@ glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc
   std::memcpy(host_job + t->off_begin, begin, sizeof(begin));
   std::memcpy(host_job + t->off_cert, cert_begin, sizeof(cert_begin));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (cudaMalloc(&t->d_job, job_bytes) != cudaSuccess || cudaMalloc(&t->d_meta, n * sizeof(uint4)) != cudaSuccess ||
-      cudaMalloc(&t->d_dconst, sizeof(dconst)) != cudaSuccess ||
-      cudaMalloc(&t->d_counters, 4 * sizeof(unsigned int)) != cudaSuccess)
-    return fail(set_error(GLC_ERR_CUDA, "tape allocation failed"));
+  if (n > t->meta_alloc) {
+    if (t->d_meta) cudaFree(t->d_meta);
+    t->d_meta = nullptr;
+    t->meta_alloc = 0;
+    if (cudaMalloc(&t->d_meta, n * sizeof(uint4)) != cudaSuccess)
+      return set_error(GLC_ERR_CUDA, "tape allocation failed");
+    t->meta_alloc = n;
+  }
+  if ((!t->d_job && cudaMalloc(&t->d_job, job_bytes) != cudaSuccess) ||
+      (!t->d_dconst && cudaMalloc(&t->d_dconst, sizeof(dconst)) != cudaSuccess) ||
+      (!t->d_counters && cudaMalloc(&t->d_counters, 4 * sizeof(unsigned int)) != cudaSuccess))
+    return set_error(GLC_ERR_CUDA, "tape allocation failed");
   // pageable sources: both copies have consumed their bytes when they return
   if (cudaMemcpyAsync(t->d_job, host_job, job_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(t->d_dconst, dconst, sizeof(dconst), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return fail(set_error(GLC_ERR_CUDA, "tape upload failed"));
+    return set_error(GLC_ERR_CUDA, "tape upload failed");
   // checkpoint slots for 512 accepted steps; when a ray needs more, the pass runs again with the
   // capacity its longest ray needs
   s = size_checkpoints(t, uint32_t(512 / t->K + 2));
   if (s == GLC_OK) s = forward(t, *out, st);
-  if (s != GLC_OK) return fail(s);
+  if (s != GLC_OK) return s;
   unsigned int counters[4];
   if (cudaMemcpyAsync(counters, t->d_counters, sizeof(counters), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
-    return fail(set_error(GLC_ERR_CUDA, "forward pass failed"));
+    return set_error(GLC_ERR_CUDA, "forward pass failed");
   if (counters[0] > 0) {
     s = size_checkpoints(t, counters[1] / t->K + 2);
     if (s == GLC_OK) s = forward(t, *out, st);
-    if (s != GLC_OK) return fail(s);
+    if (s != GLC_OK) return s;
+  }
+  return GLC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc_camera* camera, int32_t K,
+                            const glc_results* out, void* stream, glc_tape** tape) {
+  if (!ctx || !as || !camera || !out || !tape) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  *tape = nullptr;
+  DeviceScope scope(ctx->device);
+  glc_tape* t = new glc_tape();
+  const glc_status s = fill_tape(t, ctx, as, camera, K, out, stream);
+  if (s != GLC_OK) {
+    free_tape(t);
+    return s;
   }
   *tape = t;
   return GLC_OK;
+}
+
+glc_status glc_forward_ckpt_into(glc_ctx* ctx, const glc_adjoint_scene* as, const glc_camera* camera, int32_t K,
+                                 const glc_results* out, void* stream, glc_tape* tape) {
+  if (!ctx || !as || !camera || !out || !tape) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (tape->ctx != ctx) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape belongs to another context");
+  DeviceScope scope(ctx->device);
+  return fill_tape(tape, ctx, as, camera, K, out, stream);
 }
 
 glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, void* stream) {

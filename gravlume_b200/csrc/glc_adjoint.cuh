@@ -93,9 +93,10 @@ GLC_HD void dp5_stage_points(const KN<double>& k, const double y0[6], double E, 
   }
 }
 
-// kbar -> Ybar += J_y^T kbar and g (E, a, Q^2) += J_p^T kbar at stage point Y.
-GLC_HD void rhs_vjp(const KN<D9>& kd, const double Y[6], double E, const double kbar[6], double ybar[6],
-                    double g[3]) {
+// kbar -> Ybar += J_y^T kbar and g (E, a, Q^2) += J_p^T kbar at stage point Y, from the full
+// 9-channel Jacobian (kept as the cross-check of rhs_vjp).
+GLC_HD void rhs_vjp_jacobian(const KN<D9>& kd, const double Y[6], double E, const double kbar[6], double ybar[6],
+                             double g[3]) {
   D9 y[6];
   for (int c = 0; c < 6; ++c) y[c] = D9::seed(Y[c], c);
   D9 d[7], r, vr;
@@ -109,9 +110,50 @@ GLC_HD void rhs_vjp(const KN<D9>& kd, const double Y[6], double E, const double 
   }
 }
 
+// The same product from 4 channels. The reduced system is Hamiltonian, F = J grad H with
+// J = [[0, I], [-I, 0]] and H = g^{mu nu} p_mu p_nu / 2 at fixed p_t = -E, so its state Jacobian is
+// J Hess(H) and J_y^T kbar = Hess(H) u with u = J^T kbar = (-kbar_p, kbar_x). Hess(H) u is the
+// derivative of grad H = (-F_p, F_x) along u: one tangent channel seeded with u. Channels 1-3 carry
+// E, a and Q^2 for the parameter part.
+using D4 = Dual<4>;
+constexpr int kVjpDir = 0, kVjpE = 1, kVjpA = 2, kVjpQ2 = 3;
+
+GLC_HD KN<D4> kn_dual_vjp(const KN<double>& k) {
+  KN<D4> o;
+  o.a = D4::seed(k.a, kVjpA);
+  o.a2 = o.a * o.a;
+  o.s = D4(k.s);
+  o.sa = o.s * o.a;
+  o.q2 = D4::seed(k.q2, kVjpQ2);
+  return o;
+}
+
+GLC_HD void rhs_vjp(const KN<D4>& kd, const double Y[6], double E, const double kbar[6], double ybar[6],
+                    double g[3]) {
+  D4 y[6];
+  for (int c = 0; c < 3; ++c) {
+    y[c] = D4(Y[c]);
+    y[c].d[kVjpDir] = -kbar[3 + c];
+    y[3 + c] = D4(Y[3 + c]);
+    y[3 + c].d[kVjpDir] = kbar[c];
+  }
+  D4 d[7], r, vr;
+  kn_rhs(kd, y, D4::seed(E, kVjpE), d, r, vr);
+  for (int c = 0; c < 3; ++c) {
+    ybar[c] -= d[3 + c].d[kVjpDir];
+    ybar[3 + c] += d[c].d[kVjpDir];
+  }
+  for (int c = 0; c < 6; ++c) {
+    const double kb = kbar[c];
+    g[0] += d[c].d[kVjpE] * kb;
+    g[1] += d[c].d[kVjpA] * kb;
+    g[2] += d[c].d[kVjpQ2] * kb;
+  }
+}
+
 // Reverse sweep over the stages of y_out = y0 + h sum_i w_i K_i, given the stage points Y:
 // lam0 = dL/dy0 from lam = dL/dy_out, g += dL/d(E, a, Q^2).
-GLC_HD void stages_reverse(const KN<D9>& kd, const double Y[7][6], double E, double h, const double w[7],
+GLC_HD void stages_reverse(const KN<D4>& kd, const double Y[7][6], double E, double h, const double w[7],
                            const double lam[6], double lam0[6], double g[3]) {
   double kb[7][6];
   for (int i = 0; i < 7; ++i)
@@ -135,7 +177,7 @@ GLC_HD void stages_reverse(const KN<D9>& kd, const double Y[7][6], double E, dou
 }
 
 // Adjoint of one accepted step from y0 with size h (stage points recomputed in binary64).
-GLC_HD void dp5_reverse(const KN<double>& k, const KN<D9>& kd, const double y0[6], double E, double h,
+GLC_HD void dp5_reverse(const KN<double>& k, const KN<D4>& kd, const double y0[6], double E, double h,
                         const double w[7], const double lam[6], double lam0[6], double g[3]) {
   double Y[7][6], K[7][6];
   dp5_stage_points(k, y0, E, h, Y, K);
@@ -204,7 +246,7 @@ GLC_HD bool terminal_reverse(const LaneScene& sc, const double y0[6], double E, 
   g[1] += mu[kChA];
   g[2] += mu[kChQ2];
   // dense output with theta* fixed (its variation is already folded into mu)
-  stages_reverse(kd, Y, E, h, w, mu, lam0, g);
+  stages_reverse(kn_dual_vjp(k), Y, E, h, w, mu, lam0, g);
   return true;
 }
 

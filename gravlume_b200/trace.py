@@ -285,6 +285,28 @@ class Tape:
         self._last = (dl, mom, rp, params)
         return {"ray_momentum": mom, "ray_params": rp, "params": params}
 
+    def forward_again(self, observation: Observation | None = None, radius: float | None = None,
+                      polar: float | None = None, azimuth: float | None = None, results: TraceResults | None = None,
+                      stream=None) -> TraceResults:
+        """The forward pass again into this tape (glc_forward_ckpt_into), keeping its device memory:
+        the same camera and K, with the scene and observer position optionally replaced (an
+        optimization step). Returns the new results (written into `results` when given)."""
+        a, cam, K = self._request
+        if observation is not None:
+            a.input = observation.scene_input()
+        if radius is not None:
+            a.observer_radius = radius
+        if polar is not None:
+            a.observer_polar = polar
+        if azimuth is not None:
+            a.observer_azimuth = azimuth
+        res = results or TraceResults(self.slots, _torch().device("cuda", self.pipeline.device))
+        rs = res.struct()
+        N.check(N.lib().glc_forward_ckpt_into(self.pipeline._h, ctypes.byref(a), ctypes.byref(cam), K,
+                                              ctypes.byref(rs), self.pipeline._stream(stream), self.handle),
+                "glc_forward_ckpt_into")
+        return res
+
     def close(self):
         if self.handle:
             N.lib().glc_tape_destroy(self.handle)
@@ -464,7 +486,9 @@ class TracePipeline:
         h = ctypes.c_void_p()
         N.check(N.lib().glc_forward_ckpt(self._h, ctypes.byref(a), ctypes.byref(cam), int(K), ctypes.byref(rs),
                                          self._stream(stream), ctypes.byref(h)), "glc_forward_ckpt")
-        return res, Tape(h, self, slots, keep)
+        tape = Tape(h, self, slots, keep)
+        tape._request = (a, cam, int(K))
+        return res, tape
 
     def trace_image(self, observation: Observation, subpixel=(0.5, 0.5), stream=None, **kw) -> TraceResults:
         sc = observation.packed

@@ -356,6 +356,14 @@ typedef struct glc_grads {
  * checkpoints). */
 glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* scene, const glc_camera* camera, int32_t K,
                             const glc_results* out, void* stream, glc_tape** tape);
+/* The forward pass again, into a tape from glc_forward_ckpt on the same context: the tape's device
+ * memory is kept and grows only where this request needs more rays or checkpoint slots, so an
+ * optimization loop (forward, backward, parameter update) allocates nothing after its first
+ * iteration. Earlier checkpoints are overwritten, so the earlier pass's gradients are no longer
+ * available; issue it on the stream of the tape's last glc_backward (or synchronize first).
+ * Synchronizes the stream once, as glc_forward_ckpt. */
+glc_status glc_forward_ckpt_into(glc_ctx* ctx, const glc_adjoint_scene* scene, const glc_camera* camera, int32_t K,
+                                 const glc_results* out, void* stream, glc_tape* tape);
 /* Backward pass: dL_dobs is device, slots x 4 (dL/d source radius, g, escape theta, escape phi;
  * rays that end elsewhere get zero gradients). Replays each checkpointed segment and sweeps it in
  * reverse (binary64). Asynchronous on the stream. */

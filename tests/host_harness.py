@@ -87,3 +87,17 @@ def surface_radiance(model, i6, t6, r, g, slab=None):
     tau, s, ts = slab if slab is not None else (0.0, 0.0, 0.0)
     out = np.zeros(5)
     return out if f(int(model), i6, t6, 1 if slab is not None else 0, tau, s, ts, r, g, out.ctypes.data) else None
+
+
+def rhs_vjp_pair(scene, y, E, kbar):
+    """(n, 18): ybar and dL/d(E, a, Q^2) from the 4-channel Hamiltonian stage VJP, then from the
+    9-channel Jacobian."""
+    f = lib().host_rhs_vjp_pair
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p]
+    y = np.ascontiguousarray(y, dtype=np.float64).reshape(-1, 6)
+    E = np.ascontiguousarray(E, dtype=np.float64).reshape(-1)
+    kb = np.ascontiguousarray(kbar, dtype=np.float64).reshape(-1, 6)
+    out = np.zeros((y.shape[0], 18))
+    assert f(ctypes.byref(scene), y.shape[0], y.ctypes.data, E.ctypes.data, kb.ctypes.data, out.ctypes.data) == 0
+    return out

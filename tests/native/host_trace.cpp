@@ -73,7 +73,7 @@ template <int P>
 void adjoint(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st, double dir, const double* wobs,
              double* out) {
   const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor);
-  const KN<D9> kd = kn_dual(ls.kn);
+  const KN<D4> kd = kn_dual_vjp(ls.kn);
   for (int64_t i = 0; i < n; ++i) {
     Ray<P> ray;
     ray.init(ls, pol, st + 8 * i, dir);
@@ -177,4 +177,20 @@ extern "C" int host_surface_radiance(int model, double i6, double t6, int slab, 
   out5[1] = ob;
   for (int b = 0; b < 3; ++b) out5[2 + b] = rgb[b];
   return 1;
+}
+
+// Both stage VJPs at n states (rows of 6) with energy E and cotangents kbar (rows of 6): out rows of
+// 18 = (ybar, g) from the 4-channel Hamiltonian form, then (ybar, g) from the 9-channel Jacobian.
+extern "C" int host_rhs_vjp_pair(const glc_scene* sc, int64_t n, const double* y, const double* E,
+                                 const double* kbar, double* out) {
+  const LaneScene ls = make_lane_scene(*sc, 3.0);
+  const KN<D4> k4 = kn_dual_vjp(ls.kn);
+  const KN<D9> k9 = kn_dual(ls.kn);
+  for (int64_t i = 0; i < n; ++i) {
+    double* o = out + 18 * i;
+    for (int c = 0; c < 18; ++c) o[c] = 0.0;
+    rhs_vjp(k4, y + 6 * i, E[i], kbar + 6 * i, o, o + 6);
+    rhs_vjp_jacobian(k9, y + 6 * i, E[i], kbar + 6 * i, o + 9, o + 15);
+  }
+  return 0;
 }

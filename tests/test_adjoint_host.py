@@ -76,3 +76,24 @@ def test_adjoint_matches_finite_differences_of_the_trace(rays):
         scale = np.max(np.abs(fd[i]))
         err = np.max(np.abs(adj[i, :9] - fd[i])) / scale
         assert err <= REL, (i, int(term[i]), err, adj[i, :9], fd[i])
+
+
+def test_hamiltonian_stage_vjp_equals_the_jacobian_transpose():
+    """The sweeps' 4-channel stage VJP (F = J grad H, so J_y^T kbar = Hess(H) J^T kbar) against the
+    9-channel Jacobian transpose at seeded states along the frame's rays and random cotangents."""
+    obs = config1_observation(width=64, height=64)
+    osc, ev, sc = oracle_for(obs)
+    rng = np.random.default_rng(4)
+    px, py = rng.integers(0, 64, 64), rng.integers(0, 64, 64)
+    states, _, _, status = O.initial_rays(osc, px, py)
+    st = np.asarray(states)
+    # points along the rays, from the observer inwards (first-order moves keep them off the horizon)
+    t = rng.uniform(0.0, 40.0, (64, 1))
+    y = np.concatenate([st[:, 1:4] + t * st[:, 5:8] / np.linalg.norm(st[:, 5:8], axis=1, keepdims=True),
+                        st[:, 5:8]], axis=1)
+    kbar = rng.normal(size=(64, 6))
+    out = H.rhs_vjp_pair(sc, y, -st[:, 4], kbar)
+    a, b = out[:, :9], out[:, 9:]
+    scale = np.max(np.abs(b), axis=1, keepdims=True)
+    assert np.all(np.isfinite(a))
+    assert np.all(np.abs(a - b) <= 1e-12 * scale)

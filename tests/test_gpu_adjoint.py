@@ -145,3 +145,36 @@ def test_scene_parameter_gradients_match_oracle_central_differences(pipe, precis
           "p95", np.quantile(per_rel, 0.95))
     assert np.all(rel <= 1e-4), rel
     assert np.quantile(per_rel, 0.95) <= 1e-4
+
+
+def test_reused_tape_gives_the_fresh_tapes_gradients(pipe):
+    """glc_forward_ckpt_into: a tape reused across an optimization step (the scene's spin changed in
+    between, then changed back) gives bit-identical results and gradients to fresh tapes, without
+    growing its memory when the request fits."""
+    a, q, incl, r_obs, n = 0.9, 0.3, math.radians(60.0), 50.0, 32
+    isco = G.prograde_isco(a, q)
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED))
+    obs0, obs1 = observation(a, q, incl, r_obs, isco, n), observation(a - 0.01, q, incl, r_obs, isco, n)
+
+    def grads(tape, res):
+        w = weights(res.numpy()["termination"])
+        g = tape.backward(w)
+        torch.cuda.synchronize()
+        return res.numpy(), g["ray_momentum"].cpu().numpy(), g["params"].cpu().numpy()
+
+    fresh = []
+    for o in (obs0, obs1):
+        res, tape = pipe.forward_ckpt(o, r_obs, incl, K=16)
+        fresh.append(grads(tape, res))
+        tape.close()
+    res, tape = pipe.forward_ckpt(obs0, r_obs, incl, K=16)
+    grads(tape, res)
+    before = tape.info()["bytes"]
+    for o, want in ((obs1, fresh[1]), (obs0, fresh[0])):
+        got = grads(tape, tape.forward_again(o))
+        np.testing.assert_array_equal(got[0]["termination"], want[0]["termination"])
+        np.testing.assert_array_equal(got[0]["source_radius"], want[0]["source_radius"])
+        np.testing.assert_array_equal(got[1], want[1])
+        np.testing.assert_array_equal(got[2], want[2])
+    assert tape.info()["bytes"] == before
+    tape.close()
