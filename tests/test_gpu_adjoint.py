@@ -149,8 +149,8 @@ def test_scene_parameter_gradients_match_oracle_central_differences(pipe, precis
 
 def test_reused_tape_gives_the_fresh_tapes_gradients(pipe):
     """glc_forward_ckpt_into: a tape reused across an optimization step (the scene's spin changed in
-    between, then changed back) gives bit-identical results and gradients to fresh tapes, without
-    growing its memory when the request fits."""
+    between, then changed back) gives bit-identical results and per-ray gradients to fresh tapes, and
+    does not grow its memory when the request fits."""
     a, q, incl, r_obs, n = 0.9, 0.3, math.radians(60.0), 50.0, 32
     isco = G.prograde_isco(a, q)
     pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED))
@@ -175,6 +175,7 @@ def test_reused_tape_gives_the_fresh_tapes_gradients(pipe):
         np.testing.assert_array_equal(got[0]["termination"], want[0]["termination"])
         np.testing.assert_array_equal(got[0]["source_radius"], want[0]["source_radius"])
         np.testing.assert_array_equal(got[1], want[1])
-        np.testing.assert_array_equal(got[2], want[2])
+        # the scene gradient is summed over rays by atomics, in no fixed order
+        np.testing.assert_allclose(got[2], want[2], rtol=1e-13)
     assert tape.info()["bytes"] == before
     tape.close()
