@@ -91,8 +91,9 @@ struct LaneScene {
   double shell_r;     // MIXED binary64 shell radius
   double frequency;
   uint32_t installed; // event bits installed
-  int emission_model;  // surface transport: 0 bolometric, 1 blackbody
-  double intensity_at_six, temperature_at_six, slab_transmittance, slab_emission, slab_bands[3];
+  // the packed scene, for the surface-transport constants: read once per surface hit, so that
+  // they do not occupy registers through the stepping loop
+  const glc_scene* src;
 };
 
 GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor) {
@@ -108,12 +109,7 @@ GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor) {
   ls.surf_out = s.surface_outer;
   ls.shell_r = shell_factor * s.photon_shell_radius;
   ls.frequency = s.frequency;
-  ls.emission_model = s.emission_model;
-  ls.intensity_at_six = s.intensity_at_six;
-  ls.temperature_at_six = s.temperature_at_six;
-  ls.slab_transmittance = s.slab_transmittance;
-  ls.slab_emission = s.slab_emission;
-  for (int b = 0; b < 3; ++b) ls.slab_bands[b] = s.slab_bands[b];
+  ls.src = &s;
   ls.installed = (1u << kEvGuard) | (s.has_horizon ? 1u << kEvHorizon : 0u) | (s.has_surface ? 1u << kEvSurface : 0u) |
                  (s.has_escape ? 1u << kEvEscape : 0u);
   return ls;
@@ -868,8 +864,9 @@ struct Ray {
         res.g = g;
         // post-hit transport in binary64 (surface.rs:12-72)
         double em, ob, rgb[3];
-        if (surface_radiance(sc.emission_model, sc.intensity_at_six, sc.temperature_at_six, sc.slab_transmittance,
-                             sc.slab_emission, sc.slab_bands, double(rr), double(g), em, ob, rgb)) {
+        const glc_scene& sp = *sc.src;
+        if (surface_radiance(sp.emission_model, sp.intensity_at_six, sp.temperature_at_six, sp.slab_transmittance,
+                             sp.slab_emission, sp.slab_bands, double(rr), double(g), em, ob, rgb)) {
           res.emitted = em;
           res.observed = ob;
           for (int b = 0; b < 3; ++b) res.rgb[b] = rgb[b];
