@@ -277,7 +277,18 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
     const double r = kn_radius(ls.kn, double(ray.ys(0)), double(ray.ys(1)), double(ray.ys(2)), gs);
     reinterpret_cast<double2*>(o.position_zr)[slot] = make_double2(double(ray.ys(2)), r);
   }
-  write_radiance(o, slot, res.emitted, res.observed, res.rgb);
+  // post-hit transport (surface.rs:12-72) after the stepping loop: a function of the hit radius and
+  // g alone, evaluated where the loop's state is no longer live
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  double emitted = nan, observed = nan, rgb[3] = {0.0, 0.0, 0.0};
+  if ((o.intensity || o.radiance) && res.termination == GLC_TERM_SURFACE && isfinite(double(res.g))) {
+    const glc_scene& sp = *ls.src;
+    if (!surface_radiance(sp.emission_model, sp.intensity_at_six, sp.temperature_at_six, sp.slab_transmittance,
+                          sp.slab_emission, sp.slab_bands, double(res.surface_r), double(res.g), emitted, observed,
+                          rgb))
+      emitted = observed = nan;
+  }
+  write_radiance(o, slot, emitted, observed, rgb);
 }
 
 // A ray of a certified tile: horizon capture proven without integration (kFlagCertified); the

@@ -91,8 +91,8 @@ struct LaneScene {
   double shell_r;     // MIXED binary64 shell radius
   double frequency;
   uint32_t installed; // event bits installed
-  // the packed scene, for the surface-transport constants: read once per surface hit, so that
-  // they do not occupy registers through the stepping loop
+  // the packed scene, for the surface-transport constants: the result writer reads them after
+  // the stepping loop, so that they do not occupy registers through it
   const glc_scene* src;
 };
 
@@ -165,7 +165,6 @@ struct RayResult {
   S event_theta;  // fraction of the terminal step at the localized event (read by the adjoint)
   S escape_theta, escape_phi;
   S surface_r, surface_phi, g;
-  double emitted, observed, rgb[3];  // surface transport (valid when observed is finite)
 };
 
 // Dense output of one step as four polynomial coefficient vectors in T (built once from the
@@ -821,7 +820,6 @@ struct Ray {
     res.event_theta = S(NAN);
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
-    res.emitted = res.observed = NAN;
   }
 
   // Terminal observables at the committed event state y (precision S; binary64 in MIXED).
@@ -840,7 +838,6 @@ struct Ray {
     res.event_residual = residual;
     res.escape_theta = res.escape_phi = S(NAN);
     res.surface_r = res.surface_phi = res.g = S(NAN);
-    res.emitted = res.observed = NAN;
     if (term == GLC_TERM_ESCAPE) {
       T d[7], rr, vv;
       kn_rhs(kt, ye, E, d, rr, vv);
@@ -862,15 +859,6 @@ struct Ray {
         res.surface_r = rr;
         res.surface_phi = phi;
         res.g = g;
-        // post-hit transport in binary64 (surface.rs:12-72)
-        double em, ob, rgb[3];
-        const glc_scene& sp = *sc.src;
-        if (surface_radiance(sp.emission_model, sp.intensity_at_six, sp.temperature_at_six, sp.slab_transmittance,
-                             sp.slab_emission, sp.slab_bands, double(rr), double(g), em, ob, rgb)) {
-          res.emitted = em;
-          res.observed = ob;
-          for (int b = 0; b < 3; ++b) res.rgb[b] = rgb[b];
-        }
       } else {
         flags |= kFlagSurfaceInvalid;
       }
