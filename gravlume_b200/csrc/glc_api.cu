@@ -185,7 +185,7 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
   } else {
     const unsigned long long grid = (job.total + block - 1) / block;
     if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
-    trace_simple_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out);
+    trace_simple_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, 0ull);
     ctx->stats.last_grid = unsigned(grid);
     ctx->stats.kernel_launches += 1;
   }
@@ -276,6 +276,59 @@ glc_status ensure_job_capacity(glc_ctx* ctx, size_t bytes) {
     GLC_CUDA(cudaMallocHost(&ctx->h_stage, bytes));
     ctx->h_stage_bytes = bytes;
   }
+  return GLC_OK;
+}
+
+// A band of a host-buffer trace: rays [g0, g1) of the job, whose results fill slots [s0, s1).
+struct Band {
+  unsigned long long g0, g1, s0, s1;
+};
+
+constexpr int kMaxBands = 64;
+constexpr unsigned long long kBandRays = 1ull << 20;  // split cameras of more than this many rays
+
+// Row bands of whole tile rows for image cameras (a tile row's results are whole pixel rows, so a
+// band's slots are contiguous), equal pieces for ray lists; at most 8 bands a camera.
+bool plan_bands(const glc_camera* cams, int32_t n_cams, const JobLayout& L, const glc_policy& pol,
+                std::vector<Band>& bands) {
+  bands.clear();
+  for (int c = 0; c < n_cams; ++c) {
+    const unsigned long long g = L.begin[c], rays = L.begin[c + 1] - g;
+    if (rays == 0) continue;
+    const unsigned long long nb = std::min<unsigned long long>(8, std::max<unsigned long long>(1, rays / kBandRays));
+    if (cams[c].kind == GLC_CAMERA_RAYLIST) {
+      for (unsigned long long k = 0; k < nb; ++k) {
+        const unsigned long long j0 = rays * k / nb, j1 = rays * (k + 1) / nb;
+        bands.push_back({g + j0, g + j1, cams[c].result_offset + j0, cams[c].result_offset + j1});
+      }
+    } else {
+      const unsigned long long W = cams[c].width, H = cams[c].height;
+      const unsigned long long tiles_x = (W + pol.tile_w - 1) / pol.tile_w, tile_rows = (H + pol.tile_h - 1) / pol.tile_h;
+      const unsigned long long row_rays = tiles_x * pol.tile_w * pol.tile_h;
+      const unsigned long long per = (tile_rows + nb - 1) / nb;
+      for (unsigned long long r0 = 0; r0 < tile_rows; r0 += per) {
+        const unsigned long long r1 = std::min(r0 + per, tile_rows);
+        bands.push_back({g + r0 * row_rays, g + r1 * row_rays, cams[c].result_offset + r0 * pol.tile_h * W,
+                         cams[c].result_offset + std::min(r1 * pol.tile_h, H) * W});
+      }
+    }
+  }
+  return int(bands.size()) <= kMaxBands;
+}
+
+template <int P>
+void launch_band(const JobView& job, const glc_policy& pol, const glc_results& out, const Band& b, cudaStream_t st) {
+  JobView jb = job;
+  jb.total = b.g1;  // rays past the band's end return at once
+  const unsigned long long grid = (b.g1 - b.g0 + pol.block_threads - 1) / pol.block_threads;
+  trace_simple_kernel<P><<<unsigned(grid), pol.block_threads, 0, st>>>(jb, pol, out, b.g0);
+}
+
+glc_status ensure_host_streams(glc_ctx* ctx) {
+  if (!ctx->host_compute) GLC_CUDA(cudaStreamCreateWithFlags(&ctx->host_compute, cudaStreamNonBlocking));
+  if (!ctx->host_copy) GLC_CUDA(cudaStreamCreateWithFlags(&ctx->host_copy, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : ctx->host_band)
+    if (!e) GLC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return GLC_OK;
 }
 
@@ -459,6 +512,10 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_shadow) cudaFree(ctx->d_shadow);
   if (ctx->d_footprint) cudaFree(ctx->d_footprint);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
+  for (cudaEvent_t e : ctx->host_band)
+    if (e) cudaEventDestroy(e);
+  if (ctx->host_compute) cudaStreamDestroy(ctx->host_compute);
+  if (ctx->host_copy) cudaStreamDestroy(ctx->host_copy);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
   return GLC_OK;
@@ -677,7 +734,69 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     GLC_CUDA(cudaMalloc(&ctx->d_host_ws, bytes));
     ctx->d_host_ws_bytes = bytes;
   }
+  glc_results dev{};
+  void** dfields[kFields] = {(void**)&dev.code,    (void**)&dev.branch,  (void**)&dev.escape,  (void**)&dev.surface,
+                             (void**)&dev.redshift_time, (void**)&dev.event, (void**)&dev.drift_a,
+                             (void**)&dev.drift_b, (void**)&dev.turning, (void**)&dev.position_xy,
+                             (void**)&dev.position_zr, (void**)&dev.intensity, (void**)&dev.radiance};
+  for (int i = 0; i < kFields; ++i) *dfields[i] = hfields[i] ? ctx->d_host_ws + field_off[i] : nullptr;
   std::vector<glc_camera> cams(cameras, cameras + n_cameras);
+
+  // One-thread-per-ray launches without the pre-passes are traced in bands on one stream while the
+  // finished bands' results are copied back on another, so that the copies overlap the tracing.
+  const glc_policy& pol = ctx->policy;
+  JobLayout L;
+  std::vector<Band> bands;
+  const bool banded = pol.persistent == 0 && !pol.capture_certificates && !pol.escape_map &&
+                      validate_job(scenes, n_scenes, cameras, n_cameras, pol, L) == GLC_OK &&
+                      plan_bands(cameras, n_cameras, L, pol, bands) && bands.size() > 1;
+  if (banded) {
+    s = ensure_host_streams(ctx);
+    if (s != GLC_OK) return s;
+    cudaStream_t cs = ctx->host_compute, ps = ctx->host_copy;
+    for (int i = 0; i < n_cameras; ++i) {
+      if (cams[i].kind == GLC_CAMERA_RAYLIST && cams[i].n_rays > 0) {
+        unsigned char* d = ctx->d_host_ws + state_off[i];
+        GLC_CUDA(cudaMemcpyAsync(d, cameras[i].ray_states, cams[i].n_rays * 8 * sizeof(double),
+                                 cudaMemcpyHostToDevice, cs));
+        cams[i].ray_states = reinterpret_cast<const double*>(d);
+      }
+    }
+    s = ensure_job_capacity(ctx, L.bytes);
+    if (s != GLC_OK) return s;
+    fill_staging(ctx->h_stage, L, scenes, n_scenes, cams.data(), n_cameras);
+    GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, cs));
+    GLC_CUDA(cudaEventRecord(ctx->stage_free, cs));
+    ctx->stage_pending = true;
+    const JobView job = job_view(ctx->d_job, L, n_cameras);
+    for (size_t k = 0; k < bands.size(); ++k) {
+      switch (pol.precision) {
+        case GLC_FP32: launch_band<kFP32>(job, pol, dev, bands[k], cs); break;
+        case GLC_MIXED: launch_band<kMIXED>(job, pol, dev, bands[k], cs); break;
+        default: launch_band<kFP64>(job, pol, dev, bands[k], cs); break;
+      }
+      GLC_CUDA(cudaGetLastError());
+      GLC_CUDA(cudaEventRecord(ctx->host_band[k], cs));
+      ctx->stats.kernel_launches += 1;
+    }
+    for (size_t k = 0; k < bands.size(); ++k) {
+      GLC_CUDA(cudaStreamWaitEvent(ps, ctx->host_band[k], 0));
+      const Band& b = bands[k];
+      for (int i = 0; i < kFields; ++i) {
+        if (!hfields[i]) continue;
+        GLC_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(hfields[i]) + b.s0 * esize[i],
+                                 static_cast<unsigned char*>(*dfields[i]) + b.s0 * esize[i], (b.s1 - b.s0) * esize[i],
+                                 cudaMemcpyDeviceToHost, ps));
+      }
+    }
+    ctx->stats.last_block = pol.block_threads;
+    ctx->stats.last_persistent = 0;
+    ctx->stats.last_rays = L.total;
+    GLC_CUDA(cudaStreamSynchronize(ps));
+    GLC_CUDA(cudaStreamSynchronize(cs));
+    return GLC_OK;
+  }
+
   for (int i = 0; i < n_cameras; ++i) {
     if (cams[i].kind == GLC_CAMERA_RAYLIST && cams[i].n_rays > 0) {
       unsigned char* d = ctx->d_host_ws + state_off[i];
@@ -686,12 +805,6 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
       cams[i].ray_states = reinterpret_cast<const double*>(d);
     }
   }
-  glc_results dev{};
-  void** dfields[kFields] = {(void**)&dev.code,    (void**)&dev.branch,  (void**)&dev.escape,  (void**)&dev.surface,
-                             (void**)&dev.redshift_time, (void**)&dev.event, (void**)&dev.drift_a,
-                             (void**)&dev.drift_b, (void**)&dev.turning, (void**)&dev.position_xy,
-                             (void**)&dev.position_zr, (void**)&dev.intensity, (void**)&dev.radiance};
-  for (int i = 0; i < kFields; ++i) *dfields[i] = hfields[i] ? ctx->d_host_ws + field_off[i] : nullptr;
   s = glc_trace(ctx, scenes, n_scenes, cams.data(), n_cameras, &dev, nullptr);
   if (s != GLC_OK) return s;
   for (int i = 0; i < kFields; ++i) {

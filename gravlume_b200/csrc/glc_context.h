@@ -28,6 +28,9 @@ struct glc_ctx {
   uint32_t* d_footprint = nullptr;     // surface-footprint pixel list: counter word pair, then u64 entries
   size_t d_footprint_words = 0;
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
+  cudaStream_t host_compute = nullptr; // glc_trace_host: bands are traced on one stream ...
+  cudaStream_t host_copy = nullptr;    // ... and copied back on another
+  cudaEvent_t host_band[64] = {};      // band k traced
   size_t d_host_ws_bytes = 0;
   glc_launch_stats stats{};
 };

@@ -387,8 +387,9 @@ __device__ __forceinline__ void trace_one(const JobView& job, const glc_policy& 
 
 // One thread per ray; rays in tile order so a warp covers a compact pixel tile.
 template <int P>
-__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out) {
-  trace_one<P>(job, pol, out, (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out,
+                                                                                       unsigned long long base) {
+  trace_one<P>(job, pol, out, base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Work-queue kernel with warp-granular grabs: a grid of SMs x occupancy whose warps take
