@@ -395,6 +395,10 @@ def run_gpu(args) -> None:
         line["sky"] = sky_study(G, local)
     if args.footprint:
         line["footprint"] = footprint_study(G, local, args.cpu_sample > 0)
+    if args.scenes:
+        line["scenes"] = scenes_study(G, local, args.cpu_sample > 0)
+    if args.stress:
+        line["stress"] = stress_study(G, local, args.cpu_sample > 0, args.stress_side)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -626,6 +630,211 @@ def footprint_study(G, device: int, cpu: bool) -> dict:
     return out
 
 
+def timed_trace(pipe, scenes, cams, res, stream, flush, reps=2):
+    """Best CUDA-event time (ms) of reps traces of the job, L2 flushed before each."""
+    import torch
+
+    best = float("inf")
+    for _ in range(reps):
+        flush.fill_(3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pipe.trace(scenes, cams, res, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def frame_tolerance(G) -> dict:
+    """The binary32 frame policy's tolerances and step cap, for running FP64 at the same tolerance."""
+    p = G.ReferencePolicy.frame(G.Precision.FP32)
+    return {k: getattr(p, k) for k in ("position_rtol", "position_atol", "momentum_rtol", "momentum_atol",
+                                       "maximum_step")}
+
+
+SCENE_SET = [(0.0, 0.0), (0.5, 0.0), (0.9, 0.3), (0.998, 0.0), (0.6, 0.7)]
+SCENE_INCLINATIONS = [17.0, 60.0, 85.0]
+
+
+def scenes_study(G, device: int, cpu: bool) -> dict:
+    """The full-frame precision set at 1920x1080: (a, Q) in {(0,0), (0.5,0), (0.9,0.3), (0.998,0),
+    (0.6,0.7)} x inclinations {17, 60, 85} deg, observer at r = 50 M, 30 deg FOV, surface from the
+    prograde ISCO to 20 M. Per scene and precision (all three at the frame tolerance, rtol 1e-6):
+    CUDA-event Mrays/s (L2
+    flushed, best of two) and, with the CPU leg, the errors against the binary64 oracle (rtol 1e-10)
+    on 64 seeded pixels of the scene."""
+    import numpy as np
+    import torch
+
+    w, h = 1920, 1080
+    pipe = G.TracePipeline(device)
+    res = G.TraceResults(w * h, f"cuda:{device}")
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=f"cuda:{device}")
+    stream = torch.cuda.current_stream()
+    precisions = (("fp32", G.Precision.FP32), ("mixed", G.Precision.MIXED), ("fp64", G.Precision.FP64))
+    rows = []
+    for a, q in SCENE_SET:
+        isco = G.prograde_isco(a, q)
+        for incl in SCENE_INCLINATIONS:
+            obs = G.Observation.from_oblate(R_OBS, math.radians(incl), 0.0, spin=a, charge=q,
+                                            chart=G.KerrSchildChart.OUTGOING, width=w, height=h,
+                                            vertical_fov=math.radians(FOV_DEG), escape_radius=ESCAPE,
+                                            surface=G.EquatorialSurface(isco, SURFACE_OUTER),
+                                            horizon_offset=HORIZON_OFFSET)
+            sc = obs.pack()
+            cam = [G.image_camera(0, w, h)]
+            row = {"spin": a, "charge": q, "inclination_deg": incl}
+            ref = idx = None
+            if cpu:
+                import oracle as O
+
+                rng = np.random.default_rng(int(1000 * a + 100 * q + incl))
+                idx = np.sort(rng.choice(w * h, 64, replace=False))
+                osc = O.scene(mass=1.0, spin=a, charge=q, chart=1, observer_txyz=obs.observer_txyz, width=w,
+                              height=h, vertical_fov=obs.vertical_fov)
+                ev = O.events(escape_radius=ESCAPE, surface=(isco, SURFACE_OUTER), horizon_offset=HORIZON_OFFSET)
+                ref, _ = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, idx % w, idx // w,
+                                        threads=O.hardware_threads())
+            for name, prec in precisions:
+                pipe.set_policy(G.ReferencePolicy.frame(prec, **frame_tolerance(G)))
+                pipe.trace([sc], cam, res, stream=stream)
+                ms = timed_trace(pipe, [sc], cam, res, stream, flush)
+                entry = {"mrays_per_s": w * h / (ms / 1e3) / 1e6}
+                if ref is not None:
+                    entry["error_vs_oracle"] = error_report(G, res.numpy(), ref, idx)
+                row[name] = entry
+            rows.append(row)
+    pipe.close()
+    out = {"workload": f"kerr-newman-frames-{w}x{h}-15-scenes", "policy": "frame (rtol 1e-6)", "scenes": rows}
+    for name, _ in precisions:
+        out[f"{name}_mrays_per_s_range"] = [min(r[name]["mrays_per_s"] for r in rows),
+                                            max(r[name]["mrays_per_s"] for r in rows)]
+        if cpu:
+            out[f"{name}_class_mismatches"] = sum(r[name]["error_vs_oracle"]["class_mismatch"] for r in rows)
+    return out
+
+
+def pinhole_rays(scene, sx, sy):
+    """Initial states of pinhole rays through continuous image-plane points (sx, sy) (tangents along
+    image-right and image-up): the trace kernels' ray set-up evaluated in numpy."""
+    import numpy as np
+
+    R, U, A = (np.array(v[:4]) for v in (scene.image_right, scene.image_up, scene.arrival))
+    u = np.array(scene.four_velocity[:4])
+    g = np.array(scene.metric_covariant[:16]).reshape(4, 4)
+    nrm = 1.0 / np.hypot(1.0, np.hypot(sx, sy))
+    sight = (np.outer(sx, R) + np.outer(sy, U) - A) * nrm[:, None]
+    st = np.zeros((sx.size, 8))
+    st[:, :4] = np.array(scene.observer_txyz[:4])
+    st[:, 4:] = (scene.frequency * (u - sight)) @ g.T
+    return st
+
+
+def stress_study(G, device: int, cpu: bool, side: int = 4096) -> dict:
+    """Near-critical stress: a = 0.998, Q = 0.05, i = 85 deg, observer on the escape sphere at
+    r = 1000 M. The critical curve is located along 256 image directions by bisection of capture
+    against escape with the binary64 kernel at the strict policy (no surface); side^2 rays are drawn
+    with impact parameters uniform within +-0.05 M of it (seeded) and traced in each precision at the
+    frame tolerance (CUDA events), once without the surface (capture/escape classes and equatorial
+    crossings) and once with it (surface hits and g). With the CPU leg, 256 of them are traced by the
+    binary64 oracle at rtol 1e-12: class and crossing mismatches and the g error, with the distance
+    from the curve of every mismatch."""
+    import numpy as np
+    import torch
+
+    a, q, incl, r_obs, band = 0.998, 0.05, math.radians(85.0), 1000.0, 0.05
+    isco = G.prograde_isco(a, q)
+
+    def observation(surface):
+        return G.Observation.from_oblate(r_obs, incl, 0.0, spin=a, charge=q, chart=G.KerrSchildChart.OUTGOING,
+                                         width=64, height=64, vertical_fov=math.radians(FOV_DEG),
+                                         escape_radius=r_obs, surface=G.EquatorialSurface(isco, SURFACE_OUTER)
+                                         if surface else None, horizon_offset=HORIZON_OFFSET)
+
+    pipe = G.TracePipeline(device)
+    sky = observation(False)
+    sc = sky.pack()
+    pipe.set_policy(G.ReferencePolicy.strict_v1())
+    n_dirs = 256
+    psi = np.linspace(0.0, 2 * np.pi, n_dirs, endpoint=False)
+    lo, hi = np.zeros(n_dirs), np.full(n_dirs, 12.0 / r_obs)
+    for _ in range(40):
+        mid = 0.5 * (lo + hi)
+        d = pipe.trace_states(sky, pinhole_rays(sc, mid * np.cos(psi), mid * np.sin(psi))).numpy()
+        cap = d["termination"] == G.Termination.HORIZON_CROSSING
+        lo, hi = np.where(cap, mid, lo), np.where(cap, hi, mid)
+    rc = 0.5 * (lo + hi)
+    n = side * side
+    rng = np.random.default_rng(3)
+    k = rng.integers(0, n_dirs, n)
+    rho = rc[k] + rng.uniform(-1.0, 1.0, n) * band / r_obs
+    dist = (rho - rc[k]) * r_obs
+    out = {"workload": f"kerr-newman-near-critical-{side}x{side}", "spin": a, "charge": q, "inclination_deg": 85.0,
+           "observer_radius_m": r_obs, "band_m": band,
+           "policy": "frame (rtol 1e-6) for FP32 and MIXED, FP64 at the same tolerance"}
+    stream = torch.cuda.current_stream()
+    sample = np.sort(rng.choice(n, 256, replace=False))
+    tol = frame_tolerance(G)
+    # the sky variant probes the capture/escape boundary and the windings; the disk variant the
+    # surface hits (almost every ray of the band ends on the disk at this inclination)
+    for variant, surface in (("sky", False), ("disk", True)):
+        obs = observation(surface)
+        states = pinhole_rays(obs.pack(), rho * np.cos(psi[k]), rho * np.sin(psi[k]))
+        dev_states = torch.as_tensor(states).to(f"cuda:{device}")
+        cam = [G.raylist_camera(0, dev_states.data_ptr(), n, -1.0)]
+        res = G.TraceResults(n, f"cuda:{device}")
+        ref = None
+        vo = {}
+        if cpu:
+            import oracle as O
+
+            ev = O.events(escape_radius=r_obs, surface=(isco, SURFACE_OUTER) if surface else None,
+                          horizon_offset=HORIZON_OFFSET)
+            t0 = time.perf_counter()
+            ref = O.trace_states(1.0, a, q, 1, O.custom_policy(1e-12, 1e-14), ev, states[sample], -1.0,
+                                 threads=O.hardware_threads())
+            vo["cpu_oracle_s"] = time.perf_counter() - t0
+        for name, prec in (("fp32", G.Precision.FP32), ("mixed", G.Precision.MIXED), ("fp64", G.Precision.FP64)):
+            pipe.set_policy(G.ReferencePolicy.frame(prec, **tol))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pipe.trace([obs.packed], cam, res, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            d = res.numpy()
+            entry = {"ms": ms, "mrays_per_s": n / (ms / 1e3) / 1e6,
+                     "attempts_per_ray": float((d["accepted_steps"] + d["rejected_steps"]).mean()),
+                     "class_histogram": np.bincount(d["termination"], minlength=9).tolist(),
+                     "max_equatorial_crossings": int(d["equatorial_crossings"].max())}
+            if ref is not None:
+                import oracle as O
+
+                F = O.F
+                ot = ref[:, F["termination"]].astype(int)
+                cls = d["termination"][sample] != ot
+                wind = (~cls) & (d["equatorial_crossings"][sample] != ref[:, F["equatorial_crossings"]])
+                g_rel = None
+                srf = np.flatnonzero((~cls) & (ot == 7))
+                if srf.size:
+                    # the oracle's surface observable at its own hit state (surface.rs:12-146)
+                    g_ref = np.array([O.surface_observable(1.0, a, q, 1, isco, SURFACE_OUTER,
+                                                           ref[i, F["t"]:F["p_z"] + 1])[1][2] for i in srf])
+                    ok = np.isfinite(g_ref) & np.isfinite(d["frequency_ratio"][sample][srf])
+                    if ok.any():
+                        g_rel = float(np.max(np.abs(d["frequency_ratio"][sample][srf][ok] - g_ref[ok]) / g_ref[ok]))
+                entry["oracle_sample"] = {
+                    "rays": int(sample.size), "class_mismatch": int(cls.sum()), "crossing_mismatch": int(wind.sum()),
+                    "mismatch_distance_m": [float(x) for x in np.sort(np.abs(dist[sample][cls | wind]))],
+                    "g_rel": g_rel}
+            vo[name] = entry
+        out[variant] = vo
+        del res, dev_states
+    pipe.close()
+    return out
+
+
 def adjoint_study(G, args, device: int) -> dict:
     """Discrete adjoint throughput on the differentiation workload: 1024x1024 rays, a = 0.9, Q = 0.3,
     i = 60 deg, r_obs = 50 M, MIXED forward. The loss is the sum of squared g and hit-radius residuals
@@ -723,6 +932,11 @@ def main() -> None:
                     help="skip the tolerance sweep of the precision study")
     ap.add_argument("--no-footprint", dest="footprint", action="store_false",
                     help="skip the surface-footprint study")
+    ap.add_argument("--no-scenes", dest="scenes", action="store_false",
+                    help="skip the 15-scene full-frame precision study")
+    ap.add_argument("--no-stress", dest="stress", action="store_false",
+                    help="skip the near-critical stress study")
+    ap.add_argument("--stress-side", type=int, default=4096, help="the stress study traces side^2 rays")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-scene batch study (persistent launch, graph, autotuner)")
     ap.add_argument("--adjoint-k", type=int, nargs="+", default=[16, 64, 256])
