@@ -329,6 +329,7 @@ glc_status ensure_host_streams(glc_ctx* ctx) {
   if (!ctx->host_copy) GLC_CUDA(cudaStreamCreateWithFlags(&ctx->host_copy, cudaStreamNonBlocking));
   for (cudaEvent_t& e : ctx->host_band)
     if (!e) GLC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!ctx->host_entry) GLC_CUDA(cudaEventCreateWithFlags(&ctx->host_entry, cudaEventDisableTiming));
   return GLC_OK;
 }
 
@@ -514,6 +515,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   for (cudaEvent_t e : ctx->host_band)
     if (e) cudaEventDestroy(e);
+  if (ctx->host_entry) cudaEventDestroy(ctx->host_entry);
   if (ctx->host_compute) cudaStreamDestroy(ctx->host_compute);
   if (ctx->host_copy) cudaStreamDestroy(ctx->host_copy);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
@@ -754,6 +756,11 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     s = ensure_host_streams(ctx);
     if (s != GLC_OK) return s;
     cudaStream_t cs = ctx->host_compute, ps = ctx->host_copy;
+    // the banded streams do not synchronize with the legacy default stream; an event recorded there
+    // (which completes after all earlier work of blocking streams) orders this call after earlier
+    // traces of the context, as the one-launch path on the legacy stream is ordered
+    GLC_CUDA(cudaEventRecord(ctx->host_entry, nullptr));
+    GLC_CUDA(cudaStreamWaitEvent(cs, ctx->host_entry, 0));
     for (int i = 0; i < n_cameras; ++i) {
       if (cams[i].kind == GLC_CAMERA_RAYLIST && cams[i].n_rays > 0) {
         unsigned char* d = ctx->d_host_ws + state_off[i];

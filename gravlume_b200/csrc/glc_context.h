@@ -31,6 +31,7 @@ struct glc_ctx {
   cudaStream_t host_compute = nullptr; // glc_trace_host: bands are traced on one stream ...
   cudaStream_t host_copy = nullptr;    // ... and copied back on another
   cudaEvent_t host_band[64] = {};      // band k traced
+  cudaEvent_t host_entry = nullptr;    // orders a banded host trace after the legacy stream's work
   size_t d_host_ws_bytes = 0;
   glc_launch_stats stats{};
 };
