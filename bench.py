@@ -396,6 +396,7 @@ def run_gpu(args) -> None:
     if args.footprint:
         line["footprint"] = footprint_study(G, local, args.cpu_sample > 0)
     if args.scenes:
+        line["config1"] = config1_study(G, local, args.cpu_sample > 0)
         line["scenes"] = scenes_study(G, local, args.cpu_sample > 0)
     if args.stress:
         line["stress"] = stress_study(G, local, args.cpu_sample > 0, args.stress_side)
@@ -715,6 +716,55 @@ def scenes_study(G, device: int, cpu: bool) -> dict:
     return out
 
 
+def config1_study(G, device: int, cpu: bool) -> dict:
+    """The reference's CPU-runnable case: 256x256 pinhole, a = 0.9, Q = 0.3, i = 75 deg, r = 50 M,
+    30 deg FOV, escape 1000 M, capture at r_+ + 1e-3, surface from the prograde ISCO to 20 M. FP64 at
+    the oracle's policy (rtol 1e-10, atol 1e-12) and the three precisions at the frame tolerance:
+    CUDA-event Mrays/s (best of three) and, with the CPU leg, errors against the binary64 oracle
+    on 1024 seeded pixels."""
+    import numpy as np
+    import torch
+
+    w = h = 256
+    obs = make_observation(G, w, h)
+    sc = obs.pack()
+    cam = [G.image_camera(0, w, h)]
+    pipe = G.TracePipeline(device)
+    res = G.TraceResults(w * h, f"cuda:{device}")
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=f"cuda:{device}")
+    stream = torch.cuda.current_stream()
+    ref = idx = None
+    out = {"workload": "kerr-newman-frame-256x256"}
+    if cpu:
+        import oracle as O
+
+        idx = np.sort(np.random.default_rng(1).choice(w * h, 1024, replace=False))
+        osc = O.scene(mass=1.0, spin=SPIN, charge=CHARGE, chart=1, observer_txyz=obs.observer_txyz, width=w,
+                      height=h, vertical_fov=obs.vertical_fov)
+        ev = O.events(escape_radius=ESCAPE, surface=(obs.surface.inner_radius, SURFACE_OUTER),
+                      horizon_offset=HORIZON_OFFSET)
+        threads = O.hardware_threads()
+        t0 = time.perf_counter()
+        ref, _ = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, idx % w, idx // w, threads=threads)
+        out["cpu_oracle"] = {"mrays_per_s": idx.size / (time.perf_counter() - t0) / 1e6, "cores": threads,
+                             "sample": "1024 seeded pixels, binary64 rtol 1e-10 atol 1e-12"}
+    tol = frame_tolerance(G)
+    runs = (("fp64_oracle_policy", G.ReferencePolicy.frame(G.Precision.FP64)),
+            ("fp32", G.ReferencePolicy.frame(G.Precision.FP32, **tol)),
+            ("mixed", G.ReferencePolicy.frame(G.Precision.MIXED, **tol)),
+            ("fp64", G.ReferencePolicy.frame(G.Precision.FP64, **tol)))
+    for name, pol in runs:
+        pipe.set_policy(pol)
+        pipe.trace([sc], cam, res, stream=stream)
+        ms = timed_trace(pipe, [sc], cam, res, stream, flush, reps=3)
+        entry = {"ms": ms, "mrays_per_s": w * h / (ms / 1e3) / 1e6}
+        if ref is not None:
+            entry["error_vs_oracle"] = error_report(G, res.numpy(), ref, idx)
+        out[name] = entry
+    pipe.close()
+    return out
+
+
 def pinhole_rays(scene, sx, sy):
     """Initial states of pinhole rays through continuous image-plane points (sx, sy) (tangents along
     image-right and image-up): the trace kernels' ray set-up evaluated in numpy."""
@@ -933,7 +983,7 @@ def main() -> None:
     ap.add_argument("--no-footprint", dest="footprint", action="store_false",
                     help="skip the surface-footprint study")
     ap.add_argument("--no-scenes", dest="scenes", action="store_false",
-                    help="skip the 15-scene full-frame precision study")
+                    help="skip the 256x256 and the 15-scene full-frame precision studies")
     ap.add_argument("--no-stress", dest="stress", action="store_false",
                     help="skip the near-critical stress study")
     ap.add_argument("--stress-side", type=int, default=4096, help="the stress study traces side^2 rays")
