@@ -357,3 +357,25 @@ def footprint_metrics(jacobian):
     j = _c(np.asarray(jacobian, dtype=np.float64).reshape(4), np.float64)
     out = np.zeros(4)
     return out if f(j.ctypes.data, out.ctypes.data) else None
+
+
+IND_PARAMS = ["p_t", "p_x", "p_y", "p_z", "a", "Q"]
+IND_OBS = ["source_radius", "frequency_ratio", "escape_theta", "escape_phi"]
+
+
+def ind_gradients(mass, spin, charge, chart, policy, ev, states, direction=-1.0, h_rel=1e-6, threads=1):
+    """Internal numerical differentiation of traces (the adjoint's check): per ray (termination, ok,
+    the 4 observables IND_OBS, then d(observables)/d(param) for IND_PARAMS, param-major), from central
+    differences of traces that replay the unperturbed trace's accepted step sizes."""
+    states = _c(states, np.float64).reshape(-1, 8)
+    n = states.shape[0]
+    out = np.zeros((n, 30))
+    f = lib().gro_ind_gradients
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+    rc = f(mass, spin, charge, chart, ctypes.byref(policy), ctypes.byref(ev), n, states.ctypes.data, direction, h_rel,
+           threads, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"spacetime rejected ({rc})")
+    return {"termination": out[:, 0].astype(int), "ok": out[:, 1] == 1.0, "obs": out[:, 2:6],
+            "grad": out[:, 6:].reshape(n, 6, 4)}

@@ -374,4 +374,74 @@ int gro_footprint_metrics(const double* J, double* out4) {
   return 1;
 }
 
+// Internal numerical differentiation of traces (the check of the discrete adjoint; not part of the
+// reference): for each ray, the observables (source radius and g at a surface hit with g's observer
+// frequency 1; escape polar and azimuthal angle of the coordinate direction at an escape) and their
+// central differences with respect to p_t, p_x, p_y, p_z of the initial state and to a and Q of the
+// spacetime, every perturbed trace replaying the unperturbed trace's accepted step sizes.
+// out: 30 doubles per ray = termination, ok, the 4 observables, then d(4 observables)/d(param) for
+// the 6 parameters in that order (param-major). h_rel: step relative to |p| (momenta) or absolute
+// (a, Q).
+int gro_ind_gradients(double m, double a, double q, int chart, const gro_policy* pol, const gro_events* ev, int64_t n,
+                      const double* states, double direction, double h_rel, int threads, double* out) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
+  const Policy policy = to_policy(*pol);
+  const EventConfig events = to_events(*ev);
+  auto observe = [&](const Tracer& tr, const Outcome& o, double obs[4]) {
+    for (int k = 0; k < 4; ++k) obs[k] = NAN;
+    if (o.termination == Termination::EquatorialSurface) {
+      if (tr.sp.radius(o.state, obs[0]) != GeometryError::None) return false;
+      Outcome so{};
+      if (observable_at(tr.sp, events.surface_inner, events.surface_outer, 1.0, o.state, 1.0, so) != 1) return false;
+      obs[1] = so.frequency_ratio;
+      return true;
+    }
+    if (o.termination == Termination::Escape && o.has_escape_direction) {
+      obs[2] = std::acos(std::fmax(-1.0, std::fmin(1.0, o.escape_direction[2])));
+      obs[3] = std::atan2(o.escape_direction[1], o.escape_direction[0]);
+      return true;
+    }
+    return false;
+  };
+  parallel_for(n, threads, [&](int64_t i) {
+    double* row = out + 30 * i;
+    for (int k = 0; k < 30; ++k) row[k] = 0.0;
+    const double* st = states + 8 * i;
+    const Tracer base{sp, policy, events};
+    std::vector<double> steps;
+    const Outcome o0 = base.trace(st, direction, &steps, nullptr);
+    row[0] = double(int(o0.termination));
+    double obs0[4];
+    if (!observe(base, o0, obs0)) return;
+    for (int k = 0; k < 4; ++k) row[2 + k] = obs0[k];
+    const double pn = std::sqrt(st[5] * st[5] + st[6] * st[6] + st[7] * st[7]);
+    for (int p = 0; p < 6; ++p) {
+      double d[2][4];
+      const double h = p < 4 ? h_rel * pn : h_rel;
+      for (int sgn = 0; sgn < 2; ++sgn) {
+        const double hs = sgn == 0 ? h : -h;
+        double s2[8];
+        for (int c = 0; c < 8; ++c) s2[c] = st[c];
+        Spacetime sp2 = sp;
+        if (p < 4) {
+          s2[4 + p] += hs;
+        } else if (!Spacetime::make(m, p == 4 ? a + hs : a, p == 5 ? q + hs : q, sp.chart, sp2)) {
+          return;
+        }
+        const Tracer tr{sp2, policy, events};
+        const Outcome o = tr.trace(s2, direction, nullptr, &steps);
+        if (o.termination != o0.termination || o.accepted_steps != o0.accepted_steps || !observe(tr, o, d[sgn])) return;
+      }
+      for (int k = 0; k < 4; ++k) {
+        double diff = d[0][k] - d[1][k];
+        if (k == 3) diff = std::remainder(diff, 2.0 * M_PI);
+        row[6 + 4 * p + k] = std::isfinite(diff) ? diff / (2.0 * h) : 0.0;
+      }
+    }
+    row[1] = 1.0;
+  });
+  return 0;
+}
+
 }  // extern "C"

@@ -347,7 +347,13 @@ struct Tracer {
     return r >= events.surface_inner && r <= events.surface_outer;
   }
 
-  Outcome trace(const double initial[8], double direction_sign) const;
+  // record: when given, receives the signed size of every accepted step. replay: when given, the
+  // attempts take these sizes in order and are all accepted (no error test) while the list lasts,
+  // then stepping is adaptive again. Together they give the traced map with its step sequence held
+  // fixed, whose central differences are the internal numerical differentiation of the trace
+  // (the check of the adjoint; not part of the reference).
+  Outcome trace(const double initial[8], double direction_sign, std::vector<double>* record = nullptr,
+                const std::vector<double>* replay = nullptr) const;
 };
 
 struct DenseRoot {
@@ -396,7 +402,8 @@ struct LocalizedRoot {
 };
 
 // geodesic.rs:53-506 GeodesicTracer::trace / TraceExecution
-inline Outcome Tracer::trace(const double initial[8], double sign) const {
+inline Outcome Tracer::trace(const double initial[8], double sign, std::vector<double>* record,
+                             const std::vector<double>* replay) const {
   Outcome o{};
   o.event_kind = -1;
   o.surface_status = 0;
@@ -474,6 +481,8 @@ inline Outcome Tracer::trace(const double initial[8], double sign) const {
   StepAttempt att;
   for (;;) {
     if (accepted >= policy.maximum_accepted_steps) return finish(state, Termination::StepExhaustion);
+    const bool replaying = replay != nullptr && accepted < replay->size();
+    if (replaying) step = (*replay)[accepted];
     const double mag = std::fabs(step);
     if (!have_min) {
       hmin = mag;
@@ -496,7 +505,7 @@ inline Outcome Tracer::trace(const double initial[8], double sign) const {
     es_end[0] = es_start[0] + att.dense.time_increment(1.0);
     const double en = policy.error_norm(es_start, es_end, att.error);
     if (!std::isfinite(en)) return finish_failure(NumericalFailure::NonFinite);
-    if (en > 1.0) {
+    if (!replaying && en > 1.0) {
       rejected += 1;
       consecutive += 1;
       if (consecutive >= policy.maximum_consecutive_rejects) return finish(state, Termination::RejectExhaustion);
@@ -506,6 +515,7 @@ inline Outcome Tracer::trace(const double initial[8], double sign) const {
     }
     accepted += 1;
     consecutive = 0;
+    if (record) record->push_back(step);
     for (int i = 0; i < 8; ++i)
       if (!std::isfinite(att.end[i])) return finish_failure(NumericalFailure::NonFinite);
     const double* end_state = att.end;

@@ -97,3 +97,25 @@ def test_hamiltonian_stage_vjp_equals_the_jacobian_transpose():
     scale = np.max(np.abs(b), axis=1, keepdims=True)
     assert np.all(np.isfinite(a))
     assert np.all(np.abs(a - b) <= 1e-12 * scale)
+
+
+def test_adjoint_matches_the_oracles_internal_numerical_differentiation(rays):
+    """The sweeps' gradient with respect to (p_t, p_x, p_y, p_z, a, Q) against the oracle's internal
+    numerical differentiation: central differences (h = 1e-6) of oracle traces at rtol 1e-12 that
+    replay the unperturbed trace's accepted steps, i.e. the tangent of the oracle's own discrete map.
+    The two maps take different step sequences at the same tolerance, so they agree to the
+    integration accuracy; 1e-6 of the gradient's largest component is asked."""
+    sc, pol, states, base = rays
+    obs = config1_observation(width=64, height=64)
+    osc, ev, _ = oracle_for(obs)
+    ind = O.ind_gradients(1.0, 0.9, 0.3, 1, O.custom_policy(1e-12, 1e-14), ev, states, -1.0, 1e-6,
+                          threads=O.default_threads())
+    assert ind["ok"].all()
+    term = ind["termination"]
+    w = weights(term)
+    host = H.adjoint_states(sc, pol, states, -1.0, w)
+    assert (host[:, 10] == 1.0).all()
+    adj = np.stack([-host[:, 6], host[:, 3], host[:, 4], host[:, 5], host[:, 7], 2 * 0.3 * host[:, 8]], axis=1)
+    want = np.einsum("npk,nk->np", ind["grad"], w)
+    rel = np.abs(adj - want).max(axis=1) / np.abs(want).max(axis=1)
+    assert rel.max() <= 1e-6, rel.max()

@@ -179,3 +179,44 @@ def test_reused_tape_gives_the_fresh_tapes_gradients(pipe):
         np.testing.assert_allclose(got[2], want[2], rtol=1e-13)
     assert tape.info()["bytes"] == before
     tape.close()
+
+
+@pytest.mark.parametrize("precision", [G.Precision.FP64, G.Precision.MIXED])
+def test_ray_gradients_match_the_oracles_internal_numerical_differentiation(pipe, precision):
+    """The differentiation workload's rays (a = 0.9, Q = 0.3, i = 60 deg, r = 50 M; 1024 seeded pixels
+    of the 1024x1024 frame): the device adjoint's per-ray gradients with respect to (p_t, p_x, p_y,
+    p_z) and to a and Q in the dynamics, against the oracle's internal numerical differentiation at
+    rtol 1e-12 (central differences of traces replaying the unperturbed trace's steps). The binary64
+    forward at rtol 1e-12 agrees to 1e-6 of each gradient's largest component; the MIXED forward at
+    the frame tolerance carries its rtol 1e-6 truncation, and the adjoint's precision target, 1e-4,
+    is asked of 95 % of its rays."""
+    a, q, incl, r_obs, n = 0.9, 0.3, math.radians(60.0), 50.0, 1024
+    isco = G.prograde_isco(a, q)
+    obs = observation(a, q, incl, r_obs, isco, n)
+    osc, ev, _ = oracle_for(obs)
+    rng = np.random.default_rng(40)
+    idx = np.sort(rng.choice(n * n, 1024, replace=False))
+    states, _, _, status = O.initial_rays(osc, idx % n, idx // n)
+    assert (status == 0).all()
+    states = np.asarray(states)
+    ind = O.ind_gradients(1.0, a, q, 1, O.custom_policy(1e-12, 1e-14), ev, states, -1.0, 1e-6,
+                          threads=O.hardware_threads())
+    keep = ind["ok"]
+    assert keep.mean() >= 0.95
+    w = weights(ind["termination"])
+    want = np.einsum("npk,nk->np", ind["grad"], w)
+    pipe.set_policy(tight() if precision == G.Precision.FP64 else G.ReferencePolicy.frame(G.Precision.MIXED))
+    res, tape = pipe.forward_ckpt(obs, r_obs, incl, K=64, states=states)
+    d = res.numpy()
+    g = tape.backward(w)
+    torch.cuda.synchronize()
+    got = np.concatenate([g["ray_momentum"].cpu().numpy(), g["ray_params"].cpu().numpy()[:, :2]], axis=1)
+    tape.close()
+    keep &= d["termination"] == ind["termination"]
+    rel = np.abs(got[keep] - want[keep]).max(axis=1) / np.abs(want[keep]).max(axis=1)
+    print(precision.name, "rays", int(keep.sum()), "median", float(np.median(rel)), "p95",
+          float(np.quantile(rel, 0.95)), "max", float(rel.max()))
+    if precision == G.Precision.FP64:
+        assert rel.max() <= 1e-6
+    else:
+        assert np.quantile(rel, 0.95) <= 1e-4
