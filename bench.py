@@ -312,6 +312,15 @@ def run_gpu(args) -> None:
                     TRAFFIC_BYTES_PER_RAY[args.precision] * rays if args.precision in TRAFFIC_BYTES_PER_RAY else None),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1280x720, scaled by rays",
                 "algorithmic_bytes_per_launch": float(sum(N.RESULT_BYTES.values())) * rays}
+    # the same launch against HBM, to show how far from bandwidth-bound the path is
+    hbm_peak, hbm_source = 6650.0, "fallback"
+    try:
+        hbm_peak, hbm_source = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        pass
+    hbm_achieved = roofline["algorithmic_bytes_per_launch"] / launch_s / 1e9
+    roofline["hbm_view"] = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
+                            "peak_source": f"{hbm_source} copy bandwidth"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
