@@ -184,3 +184,25 @@ def test_footprint_rejects_ray_lists_and_off_center_stencils(pipe):
     rl = [G.raylist_camera(0, states.data_ptr(), 4, -1.0)]
     with pytest.raises(G.GlcError, match="image cameras"):
         pipe.surface_footprint([sc], rl, G.TraceResults(4, "cuda"), "tangent")
+
+
+@pytest.mark.parametrize("method", ["quarter_pixel", "tangent"])
+def test_two_cameras_in_one_call_equal_separate_calls(pipe, method):
+    """Two image cameras of different scenes and sizes in one call (results at their own offsets)
+    give each camera's footprints of a call with that camera alone (binary64: per-ray results do
+    not depend on which rays share a warp)."""
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.FP64))
+    o1 = config1_observation(width=192, height=160)
+    o2 = config1_observation(width=128, height=96, spin=0.5, charge=0.0, incl_deg=60.0)
+    sc = [o1.packed, o2.packed]
+    n1, n2 = 192 * 160, 128 * 96
+    cams = [G.image_camera(0, 192, 160), G.image_camera(1, 128, 96, offset=n1 + 7)]
+    primary = G.TraceResults(n1 + 7 + n2, "cuda")
+    pipe.trace(sc, cams, primary)
+    both = G.footprint_fields(pipe.surface_footprint(sc, cams, primary, method))
+    torch.cuda.synchronize()
+    for k, (o, cam, off, n) in enumerate(((o1, cams[0], 0, n1), (o2, cams[1], n1 + 7, n2))):
+        alone, _ = footprint(pipe, o, method)
+        for name in ("jacobian", "singular_values", "determinant", "status", "parity"):
+            np.testing.assert_array_equal(both[name][off:off + n], alone[name], err_msg=f"{name} camera {k}")
+        assert (alone["status"] == G.FootprintStatus.RESOLVED).sum() > 100
