@@ -570,6 +570,33 @@ def sky_study(G, device: int) -> dict:
         out[name] = {"ms": best, "mrays_per_s": w * h / (best / 1e3) / 1e6,
                      "certified_fraction": float(((d["flags"] & 16) != 0).mean()),
                      "reconstructed_fraction": float(((d["flags"] & 32) != 0).mean())}
+    # shadow-edge refinement of the headline view without its surface (the shadow's whole rim in
+    # view): the primary trace, then glc_refine_shadow_edges, CUDA events around the refinement
+    import numpy as np
+
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED))
+    view = G.Observation.from_oblate(R_OBS, math.radians(INCL_DEG), 0.0, spin=SPIN, charge=CHARGE,
+                                     chart=G.KerrSchildChart.OUTGOING, width=WIDTH, height=HEIGHT,
+                                     vertical_fov=math.radians(FOV_DEG), escape_radius=ESCAPE, surface=None,
+                                     horizon_offset=HORIZON_OFFSET)
+    vs, vcam = view.pack(), [G.image_camera(0, WIDTH, HEIGHT)]
+    primary = G.TraceResults(WIDTH * HEIGHT, f"cuda:{device}", ["code"])
+    pipe.trace([vs], vcam, primary, stream=stream)
+    pipe.refine_shadow_edges([vs], vcam, primary, stream=stream)
+    best = float("inf")
+    for _ in range(2):
+        flush.fill_(5)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cov = pipe.refine_shadow_edges([vs], vcam, primary, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    c = cov.cpu().numpy()
+    edges = int(((c > 0) & (c < 1)).sum())
+    out["shadow_edges"] = {"workload": f"kerr-newman-sky-{WIDTH}x{HEIGHT} (headline view, no surface)",
+                           "precision": "mixed", "refine_ms": best, "fractional_coverage_pixels": edges,
+                           "escape_pixels": int((c == 1).sum()), "capture_pixels": int((c == 0).sum())}
     pipe.close()
     return out
 
