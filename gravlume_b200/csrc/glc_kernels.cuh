@@ -334,11 +334,10 @@ __device__ __forceinline__ void write_reconstructed(const glc_results& o, unsign
   write_radiance(o, slot, nan, nan, none);
 }
 
-// Register budget per precision: binary32 runs 5 blocks of 128 threads per SM (at most 102
-// registers, 20 warps; 3 % faster than 4 blocks, while 6 blocks spill enough to lose it again); the
-// binary64 and mixed kernels carry binary64 event and shell paths and run at 2 blocks per SM.
+// Register budget per precision: binary32 fits 128 registers (16 warps per SM); the binary64 and
+// mixed kernels carry binary64 event and shell paths and run at 2 blocks of 128 threads per SM.
 #ifndef GLC_MIN_BLOCKS_FP32
-#define GLC_MIN_BLOCKS_FP32 5
+#define GLC_MIN_BLOCKS_FP32 4
 #endif
 #ifndef GLC_MIN_BLOCKS_MIXED
 #define GLC_MIN_BLOCKS_MIXED 2
