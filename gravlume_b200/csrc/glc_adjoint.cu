@@ -258,6 +258,7 @@ struct glc_tape {
   size_t scratch_bytes = 0;
   unsigned int* d_counters = nullptr;
   bool pinhole = false;
+  bool valid = false;  // the last forward pass into the tape completed (backward needs it)
 
   JobView job() const {
     JobView v;
@@ -456,6 +457,7 @@ glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* as, const glc
     free_tape(t);
     return s;
   }
+  t->valid = true;
   *tape = t;
   return GLC_OK;
 }
@@ -465,11 +467,15 @@ glc_status glc_forward_ckpt_into(glc_ctx* ctx, const glc_adjoint_scene* as, cons
   if (!ctx || !as || !camera || !out || !tape) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
   if (tape->ctx != ctx) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape belongs to another context");
   DeviceScope scope(ctx->device);
-  return fill_tape(tape, ctx, as, camera, K, out, stream);
+  tape->valid = false;
+  const glc_status s = fill_tape(tape, ctx, as, camera, K, out, stream);
+  tape->valid = s == GLC_OK;
+  return s;
 }
 
 glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, void* stream) {
   if (!t || !dl || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if (!t->valid) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape's last forward pass failed; run it again");
   DeviceScope scope(t->ctx->device);
   const size_t need = size_t(t->K) * 7 * sizeof(double) * t->n;
   if (need > t->scratch_bytes) {

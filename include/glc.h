@@ -361,7 +361,8 @@ glc_status glc_forward_ckpt(glc_ctx* ctx, const glc_adjoint_scene* scene, const 
  * optimization loop (forward, backward, parameter update) allocates nothing after its first
  * iteration. Earlier checkpoints are overwritten, so the earlier pass's gradients are no longer
  * available; issue it on the stream of the tape's last glc_backward (or synchronize first).
- * Synchronizes the stream once, as glc_forward_ckpt. */
+ * Synchronizes the stream once, as glc_forward_ckpt. When it fails, glc_backward rejects the tape
+ * until a forward pass into it succeeds. */
 glc_status glc_forward_ckpt_into(glc_ctx* ctx, const glc_adjoint_scene* scene, const glc_camera* camera, int32_t K,
                                  const glc_results* out, void* stream, glc_tape* tape);
 /* Backward pass: dL_dobs is device, slots x 4 (dL/d source radius, g, escape theta, escape phi;

@@ -220,3 +220,24 @@ def test_ray_gradients_match_the_oracles_internal_numerical_differentiation(pipe
         assert rel.max() <= 1e-6
     else:
         assert np.quantile(rel, 0.95) <= 1e-4
+
+
+def test_failed_forward_into_a_tape_blocks_its_backward(pipe):
+    """A forward pass into a reused tape that the library rejects (here a view of another size than
+    the tape's camera) leaves the tape unusable for glc_backward until a forward pass succeeds."""
+    a, q, incl, r_obs, n = 0.9, 0.3, math.radians(60.0), 50.0, 16
+    isco = G.prograde_isco(a, q)
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED))
+    obs = observation(a, q, incl, r_obs, isco, n)
+    res, tape = pipe.forward_ckpt(obs, r_obs, incl, K=16)
+    w = weights(res.numpy()["termination"])
+    tape.backward(w)
+    with pytest.raises(G.GlcError, match="size"):
+        tape.forward_again(observation(a, q, incl, r_obs, isco, n + 8))
+    with pytest.raises(G.GlcError, match="failed"):
+        tape.backward(w)
+    res = tape.forward_again(obs)
+    g = tape.backward(w)
+    torch.cuda.synchronize()
+    assert np.isfinite(g["ray_momentum"].cpu().numpy()).all()
+    tape.close()
