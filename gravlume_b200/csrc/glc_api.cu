@@ -285,17 +285,17 @@ struct Band {
 };
 
 constexpr int kMaxBands = 64;
-constexpr unsigned long long kBandRays = 1ull << 20;  // split cameras of more than this many rays
+constexpr unsigned long long kBandRays = 1ull << 19;  // split cameras of more than this many rays
 
 // Row bands of whole tile rows for image cameras (a tile row's results are whole pixel rows, so a
-// band's slots are contiguous), equal pieces for ray lists; at most 8 bands a camera.
+// band's slots are contiguous), equal pieces for ray lists; at most 16 bands a camera.
 bool plan_bands(const glc_camera* cams, int32_t n_cams, const JobLayout& L, const glc_policy& pol,
                 std::vector<Band>& bands) {
   bands.clear();
   for (int c = 0; c < n_cams; ++c) {
     const unsigned long long g = L.begin[c], rays = L.begin[c + 1] - g;
     if (rays == 0) continue;
-    const unsigned long long nb = std::min<unsigned long long>(8, std::max<unsigned long long>(1, rays / kBandRays));
+    const unsigned long long nb = std::min<unsigned long long>(16, std::max<unsigned long long>(1, rays / kBandRays));
     if (cams[c].kind == GLC_CAMERA_RAYLIST) {
       for (unsigned long long k = 0; k < nb; ++k) {
         const unsigned long long j0 = rays * k / nb, j1 = rays * (k + 1) / nb;

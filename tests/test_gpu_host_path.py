@@ -1,12 +1,13 @@
 """The end-to-end host-buffer call (glc_trace_host) against the device-buffer trace of the same job.
 
 A job large enough to be traced in bands, with its results copied back band by band on a second
-stream while later bands are traced, holds a 2048x1024 pinhole frame (two row bands) and a ray
-list behind it in the result slots. Its every result array must equal the device trace's byte for
-byte, in binary32 and binary64 (the same kernel traces every ray either way). A MIXED frame is
-compared the same way: its bands start on whole tile rows, so each warp holds the same rays as in
-the one-launch trace, and its warp-wide binary64 decisions are the same. The persistent kernel,
-whose launches are not banded, goes through the one-launch path and must match as well.
+stream while later bands are traced, holds a 2048x1024 pinhole frame (four row bands of 2^19
+rays) and a ray list behind it in the result slots. Its every result array must equal the device
+trace's byte for byte, in binary32 and binary64 (the same kernel traces every ray either way). A
+MIXED frame is compared the same way: its bands start on whole tile rows, so each warp holds the
+same rays as in the one-launch trace, and its warp-wide binary64 decisions are the same. The
+persistent kernel, whose launches are not banded, goes through the one-launch path and must match
+as well.
 """
 
 import math
@@ -69,8 +70,8 @@ def test_banded_host_trace_equals_the_device_trace(pipe, job, precision):
     pipe.set_policy(G.ReferencePolicy.frame(precision))
     before = pipe.stats().kernel_launches
     compare(pipe, sc, states)
-    # one device trace, then three bands (two row bands of the frame, one of the ray list)
-    assert pipe.stats().kernel_launches - before == 1 + 3
+    # one device trace, then five bands (four row bands of the frame, one of the ray list)
+    assert pipe.stats().kernel_launches - before == 1 + 5
 
 
 def test_banded_mixed_frame_equals_the_device_trace(pipe, job):
