@@ -325,7 +325,9 @@ void launch_band(const JobView& job, const glc_policy& pol, const glc_results& o
 }
 
 glc_status ensure_host_streams(glc_ctx* ctx) {
-  if (!ctx->host_compute) GLC_CUDA(cudaStreamCreateWithFlags(&ctx->host_compute, cudaStreamNonBlocking));
+  for (cudaStream_t& c : ctx->host_compute)
+    if (!c) GLC_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+  if (!ctx->host_upload) GLC_CUDA(cudaEventCreateWithFlags(&ctx->host_upload, cudaEventDisableTiming));
   if (!ctx->host_copy) GLC_CUDA(cudaStreamCreateWithFlags(&ctx->host_copy, cudaStreamNonBlocking));
   for (cudaEvent_t& e : ctx->host_band)
     if (!e) GLC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -516,7 +518,9 @@ glc_status glc_destroy(glc_ctx* ctx) {
   for (cudaEvent_t e : ctx->host_band)
     if (e) cudaEventDestroy(e);
   if (ctx->host_entry) cudaEventDestroy(ctx->host_entry);
-  if (ctx->host_compute) cudaStreamDestroy(ctx->host_compute);
+  if (ctx->host_upload) cudaEventDestroy(ctx->host_upload);
+  for (cudaStream_t c : ctx->host_compute)
+    if (c) cudaStreamDestroy(c);
   if (ctx->host_copy) cudaStreamDestroy(ctx->host_copy);
   if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
   delete ctx;
@@ -755,7 +759,7 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
   if (banded) {
     s = ensure_host_streams(ctx);
     if (s != GLC_OK) return s;
-    cudaStream_t cs = ctx->host_compute, ps = ctx->host_copy;
+    cudaStream_t cs = ctx->host_compute[0], cs2 = ctx->host_compute[1], ps = ctx->host_copy;
     // the banded streams do not synchronize with the legacy default stream; an event recorded there
     // (which completes after all earlier work of blocking streams) orders this call after earlier
     // traces of the context, as the one-launch path on the legacy stream is ordered
@@ -775,15 +779,19 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, cs));
     GLC_CUDA(cudaEventRecord(ctx->stage_free, cs));
     ctx->stage_pending = true;
+    // bands alternate between two streams, so that one band's last warps overlap the next band
+    GLC_CUDA(cudaEventRecord(ctx->host_upload, cs));
+    GLC_CUDA(cudaStreamWaitEvent(cs2, ctx->host_upload, 0));
     const JobView job = job_view(ctx->d_job, L, n_cameras);
     for (size_t k = 0; k < bands.size(); ++k) {
+      cudaStream_t bs = (k & 1u) ? cs2 : cs;
       switch (pol.precision) {
-        case GLC_FP32: launch_band<kFP32>(job, pol, dev, bands[k], cs); break;
-        case GLC_MIXED: launch_band<kMIXED>(job, pol, dev, bands[k], cs); break;
-        default: launch_band<kFP64>(job, pol, dev, bands[k], cs); break;
+        case GLC_FP32: launch_band<kFP32>(job, pol, dev, bands[k], bs); break;
+        case GLC_MIXED: launch_band<kMIXED>(job, pol, dev, bands[k], bs); break;
+        default: launch_band<kFP64>(job, pol, dev, bands[k], bs); break;
       }
       GLC_CUDA(cudaGetLastError());
-      GLC_CUDA(cudaEventRecord(ctx->host_band[k], cs));
+      GLC_CUDA(cudaEventRecord(ctx->host_band[k], bs));
       ctx->stats.kernel_launches += 1;
     }
     for (size_t k = 0; k < bands.size(); ++k) {
@@ -801,6 +809,7 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     ctx->stats.last_rays = L.total;
     GLC_CUDA(cudaStreamSynchronize(ps));
     GLC_CUDA(cudaStreamSynchronize(cs));
+    GLC_CUDA(cudaStreamSynchronize(cs2));
     return GLC_OK;
   }
 

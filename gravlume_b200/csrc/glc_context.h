@@ -28,8 +28,9 @@ struct glc_ctx {
   uint32_t* d_footprint = nullptr;     // surface-footprint pixel list: counter word pair, then u64 entries
   size_t d_footprint_words = 0;
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
-  cudaStream_t host_compute = nullptr; // glc_trace_host: bands are traced on one stream ...
-  cudaStream_t host_copy = nullptr;    // ... and copied back on another
+  cudaStream_t host_compute[2] = {};  // glc_trace_host: bands are traced on two streams in turn ...
+  cudaStream_t host_copy = nullptr;    // ... and copied back on a third
+  cudaEvent_t host_upload = nullptr;   // the job table is on the device
   cudaEvent_t host_band[64] = {};      // band k traced
   cudaEvent_t host_entry = nullptr;    // orders a banded host trace after the legacy stream's work
   size_t d_host_ws_bytes = 0;
