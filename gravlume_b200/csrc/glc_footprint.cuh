@@ -15,6 +15,8 @@
 //    (z = 0 at the hit). One re-trace per listed pixel.
 #pragma once
 
+#include <type_traits>
+
 #include "glc_adjoint.cuh"
 #include "glc_kernels.cuh"
 
@@ -180,20 +182,19 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) footprint_qua
   }
 }
 
-// Slopes K_i, i < kStages, of the step from y0 with size h (frozen), in dual arithmetic.
-template <int kStages>
-__device__ __forceinline__ void dual_stages(const KN<double>& k, const D2 y0[6], const D2& E, double h,
-                                            D2 K[kStages][6]) {
-  const KN<D2> kt{D2(k.a), D2(k.a2), D2(k.s), D2(k.sa), D2(k.q2)};
+// Slopes K_i, i < kStages, of the step from y0 with size h (frozen), in the dual arithmetic D.
+template <int kStages, class D>
+__device__ __forceinline__ void dual_stages(const KN<double>& k, const D y0[6], const D& E, double h, D K[kStages][6]) {
+  const KN<D> kt{D(k.a), D(k.a2), D(k.s), D(k.sa), D(k.q2)};
   for (int i = 0; i < kStages; ++i) {
-    D2 Y[6];
+    D Y[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
-      D2 s(0.0);
+      D s(0.0);
       for (int j = 0; j < i; ++j) s += dp_coef(i, j) * K[j][c];
       Y[c] = y0[c] + h * s;
     }
-    D2 d[7], r, vr;
+    D d[7], r, vr;
     kn_rhs(kt, Y, E, d, r, vr);
 #pragma unroll
     for (int c = 0; c < 6; ++c) K[i][c] = d[c];
@@ -202,14 +203,15 @@ __device__ __forceinline__ void dual_stages(const KN<double>& k, const D2 y0[6],
 
 // Tangent of an accepted step: y <- y + h sum_i b_i K_i with the stages in dual arithmetic (the
 // seventh stage, the slope at the end point, has weight 0).
-__device__ __noinline__ void step_tangent(const KN<double>& k, D2 y[6], const D2& E, double h) {
-  D2 K[6][6];
+template <class D>
+__device__ __noinline__ void step_tangent(const KN<double>& k, D y[6], const D& E, double h) {
+  D K[6][6];
   dual_stages<6>(k, y, E, h, K);
   double w[7];
   step_weights(w);
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
-    D2 s(0.0);
+    D s(0.0);
 #pragma unroll
     for (int i = 0; i < 6; ++i) s += w[i] * K[i][c];
     y[c] = y[c] + h * s;
@@ -218,28 +220,38 @@ __device__ __noinline__ void step_tangent(const KN<double>& k, D2 y[6], const D2
 
 // Tangent of the state at the terminal surface event, dense-output fraction theta: y(theta) with the
 // event time moving so that z stays 0 (d theta = -dz / zdot).
-__device__ __noinline__ void hit_tangent(const KN<double>& k, D2 y[6], const D2& E, double h, double theta) {
-  D2 K[7][6];
+template <class D>
+__device__ __noinline__ void hit_tangent(const KN<double>& k, D y[6], const D& E, double h, double theta) {
+  D K[7][6];
   dual_stages<7>(k, y, E, h, K);
   double w[7], dw[7];
   dense_weights_at(theta, w, dw);
-  D2 ys[6];
+  D ys[6];
   double ydot[6];
   for (int c = 0; c < 6; ++c) {
-    D2 s(0.0);
+    D s(0.0);
     double sd = 0.0;
     for (int i = 0; i < 7; ++i) {
       s += w[i] * K[i][c];
-      sd += dw[i] * K[i][c].v;
+      sd += dw[i] * double(K[i][c].v);
     }
     ys[c] = y[c] + h * s;
     ydot[c] = h * sd;
   }
   for (int ch = 0; ch < 2; ++ch) {
-    const double dtheta = -ys[2].d[ch] / ydot[2];
-    for (int c = 0; c < 6; ++c) ys[c].d[ch] += ydot[c] * dtheta;
+    const double dtheta = -double(ys[2].d[ch]) / ydot[2];
+    for (int c = 0; c < 6; ++c) ys[c].d[ch] += decltype(ys[c].v)(ydot[c] * dtheta);
   }
   for (int c = 0; c < 6; ++c) y[c] = ys[c];
+}
+
+// A binary64 dual rounded to the dual type D.
+template <class D>
+__device__ __forceinline__ D dual_cast(const D2& x) {
+  D r(x.v);
+  r.d[0] = decltype(r.v)(x.d[0]);
+  r.d[1] = decltype(r.v)(x.d[1]);
+  return r;
 }
 
 // The set-up of image_state on the dual image point (u, v) = pixel + subpixel, seeded d/du, d/dv:
@@ -301,9 +313,17 @@ __global__ void __launch_bounds__(128, 2) footprint_tangent_kernel(
     Ray<P> ray;
     ray.init(ls, pol, st8, -1.0);
     RayResult<S> res;
-    D2 ty[6], E;
-    image_state_tangent(sc, cam, double(px) + cam.subpixel_x, double(py) + cam.subpixel_y, ty, E);
-    E.v = double(ray.E);
+    // the tangents in the trace's own stage precision: binary32 duals for FP32, binary64 otherwise
+    using D = typename std::conditional<P == kFP32, Dual<2, float>, D2>::type;
+    using R = decltype(D::v);
+    D ty[6], E;
+    {
+      D2 t2[6], e2;
+      image_state_tangent(sc, cam, double(px) + cam.subpixel_x, double(py) + cam.subpixel_y, t2, e2);
+      for (int c = 0; c < 6; ++c) ty[c] = dual_cast<D>(t2[c]);
+      E = dual_cast<D>(e2);
+    }
+    E.v = R(ray.E);
     bool hit = false;
     for (;;) {
       double y0[6];
@@ -315,14 +335,14 @@ __global__ void __launch_bounds__(128, 2) footprint_tangent_kernel(
       if (ray_step<P>(ray, ls, pol, res, use64)) {
         const uint32_t w = (res.termination & 0xFFu) | ((res.candidates & 0xFu) << 12) | ((res.flags & 0xFFFu) << 20);
         if (resolved_surface_code(w)) {
-          for (int c = 0; c < 6; ++c) ty[c].v = y0[c];
+          for (int c = 0; c < 6; ++c) ty[c].v = R(y0[c]);
           hit_tangent(ls.kn, ty, E, h0, double(res.event_theta));
           hit = true;
         }
         break;
       }
       if (ray.accepted != acc) {
-        for (int c = 0; c < 6; ++c) ty[c].v = y0[c];
+        for (int c = 0; c < 6; ++c) ty[c].v = R(y0[c]);
         step_tangent(ls.kn, ty, E, h0);
       }
     }
@@ -332,12 +352,12 @@ __global__ void __launch_bounds__(128, 2) footprint_tangent_kernel(
     }
     // source radius and oblate azimuth phi = atan2(y, x) - atan2(s a, r) at the hit (the observable's
     // own expressions), differentiated; arc = r_c dphi
-    const KN<D2> kd{D2(ls.kn.a), D2(ls.kn.a2), D2(ls.kn.s), D2(ls.kn.sa), D2(ls.kn.q2)};
+    const KN<D> kd{D(ls.kn.a), D(ls.kn.a2), D(ls.kn.s), D(ls.kn.sa), D(ls.kn.q2)};
     int gs;
-    const D2 r = kn_radius(kd, ty[0], ty[1], ty[2], gs);
-    const D2 phi = g_atan2(ty[1], ty[0]) - g_atan2(D2(ls.kn.sa), r);
+    const D r = kn_radius(kd, ty[0], ty[1], ty[2], gs);
+    const D phi = g_atan2(ty[1], ty[0]) - g_atan2(D(ls.kn.sa), r);
     const double rc = double(res.surface_r);
-    const double J[4] = {r.d[0], r.d[1], rc * phi.d[0], rc * phi.d[1]};
+    const double J[4] = {double(r.d[0]), double(r.d[1]), rc * double(phi.d[0]), rc * double(phi.d[1])};
     glc_footprint f;
     footprint_finish(J, f);
     footprint_store(out + slot, f);
