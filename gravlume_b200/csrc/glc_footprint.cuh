@@ -313,8 +313,9 @@ __global__ void __launch_bounds__(128, 2) footprint_tangent_kernel(
     Ray<P> ray;
     ray.init(ls, pol, st8, -1.0);
     RayResult<S> res;
-    // the tangents in the trace's own stage precision: binary32 duals for FP32, binary64 otherwise
-    using D = typename std::conditional<P == kFP32, Dual<2, float>, D2>::type;
+    // the tangents in the trace's own stage precision: binary32 duals for FP32 and MIXED (whose
+    // stages are binary32), binary64 for FP64
+    using D = typename std::conditional<P == kFP64, D2, Dual<2, float>>::type;
     using R = decltype(D::v);
     D ty[6], E;
     {
