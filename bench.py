@@ -949,7 +949,7 @@ def adjoint_study(G, args, device: int) -> dict:
     obs = obs_at(a, q, incl)
     stream = torch.cuda.current_stream()
     out = {"workload": f"kerr-newman-adjoint-{n}x{n}", "spin": a, "charge": q, "inclination_deg": 60.0,
-           "observer_radius_m": r_obs, "forward_precision": "mixed", "backward_precision": "f64",
+           "observer_radius_m": r_obs, "forward_precision": "mixed", "backward_precision": "f32 stage products, f64 stage points and sums",
            "target_offsets": [float(da), float(dq), float(di)], "by_K": {}}
     for K in args.adjoint_k:
         # one tape per K, reused by every step (glc_forward_ckpt_into): the steps allocate nothing

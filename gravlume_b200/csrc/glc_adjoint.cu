@@ -110,7 +110,10 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
   double rdir[3];
   ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir);
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
-  const KN<D4> kd = kn_dual_vjp(ls.kn);
+  // the reverse sweep's stage products in the forward pass's stage precision: binary32 after a
+  // MIXED forward, binary64 after an FP64 one (stage points and accumulation stay binary64)
+  using VR = typename std::conditional<P == kMIXED, float, double>::type;
+  const KN<Dual<4, VR>> kd = kn_dual_vjp<VR>(ls.kn);
   double wobs[kObs];
   bool any = false;
   for (int k = 0; k < kObs; ++k) {

@@ -118,42 +118,48 @@ GLC_HD void rhs_vjp_jacobian(const KN<D9>& kd, const double Y[6], double E, cons
 using D4 = Dual<4>;
 constexpr int kVjpDir = 0, kVjpE = 1, kVjpA = 2, kVjpQ2 = 3;
 
-GLC_HD KN<D4> kn_dual_vjp(const KN<double>& k) {
-  KN<D4> o;
-  o.a = D4::seed(k.a, kVjpA);
+// The spacetime constants with their a and Q^2 channels, over the scalar type R of the sweep.
+template <class R = double>
+GLC_HD KN<Dual<4, R>> kn_dual_vjp(const KN<double>& k) {
+  using V = Dual<4, R>;
+  KN<V> o;
+  o.a = V::seed(k.a, kVjpA);
   o.a2 = o.a * o.a;
-  o.s = D4(k.s);
+  o.s = V(k.s);
   o.sa = o.s * o.a;
-  o.q2 = D4::seed(k.q2, kVjpQ2);
+  o.q2 = V::seed(k.q2, kVjpQ2);
   return o;
 }
 
-GLC_HD void rhs_vjp(const KN<D4>& kd, const double Y[6], double E, const double kbar[6], double ybar[6],
+template <class R>
+GLC_HD void rhs_vjp(const KN<Dual<4, R>>& kd, const double Y[6], double E, const double kbar[6], double ybar[6],
                     double g[3]) {
-  D4 y[6];
+  using V = Dual<4, R>;
+  V y[6];
   for (int c = 0; c < 3; ++c) {
-    y[c] = D4(Y[c]);
-    y[c].d[kVjpDir] = -kbar[3 + c];
-    y[3 + c] = D4(Y[3 + c]);
-    y[3 + c].d[kVjpDir] = kbar[c];
+    y[c] = V(Y[c]);
+    y[c].d[kVjpDir] = R(-kbar[3 + c]);
+    y[3 + c] = V(Y[3 + c]);
+    y[3 + c].d[kVjpDir] = R(kbar[c]);
   }
-  D4 d[7], r, vr;
-  kn_rhs(kd, y, D4::seed(E, kVjpE), d, r, vr);
+  V d[7], r, vr;
+  kn_rhs(kd, y, V::seed(E, kVjpE), d, r, vr);
   for (int c = 0; c < 3; ++c) {
-    ybar[c] -= d[3 + c].d[kVjpDir];
-    ybar[3 + c] += d[c].d[kVjpDir];
+    ybar[c] -= double(d[3 + c].d[kVjpDir]);
+    ybar[3 + c] += double(d[c].d[kVjpDir]);
   }
   for (int c = 0; c < 6; ++c) {
     const double kb = kbar[c];
-    g[0] += d[c].d[kVjpE] * kb;
-    g[1] += d[c].d[kVjpA] * kb;
-    g[2] += d[c].d[kVjpQ2] * kb;
+    g[0] += double(d[c].d[kVjpE]) * kb;
+    g[1] += double(d[c].d[kVjpA]) * kb;
+    g[2] += double(d[c].d[kVjpQ2]) * kb;
   }
 }
 
 // Reverse sweep over the stages of y_out = y0 + h sum_i w_i K_i, given the stage points Y:
 // lam0 = dL/dy0 from lam = dL/dy_out, g += dL/d(E, a, Q^2).
-GLC_HD void stages_reverse(const KN<D4>& kd, const double Y[7][6], double E, double h, const double w[7],
+template <class R>
+GLC_HD void stages_reverse(const KN<Dual<4, R>>& kd, const double Y[7][6], double E, double h, const double w[7],
                            const double lam[6], double lam0[6], double g[3]) {
   double kb[7][6];
   for (int i = 0; i < 7; ++i)
@@ -176,8 +182,10 @@ GLC_HD void stages_reverse(const KN<D4>& kd, const double Y[7][6], double E, dou
   for (int c = 0; c < 6; ++c) lam0[c] = out[c];
 }
 
-// Adjoint of one accepted step from y0 with size h (stage points recomputed in binary64).
-GLC_HD void dp5_reverse(const KN<double>& k, const KN<D4>& kd, const double y0[6], double E, double h,
+// Adjoint of one accepted step from y0 with size h (stage points recomputed in binary64, the stage
+// products in the scalar type of kd).
+template <class R>
+GLC_HD void dp5_reverse(const KN<double>& k, const KN<Dual<4, R>>& kd, const double y0[6], double E, double h,
                         const double w[7], const double lam[6], double lam0[6], double g[3]) {
   double Y[7][6], K[7][6];
   dp5_stage_points(k, y0, E, h, Y, K);
