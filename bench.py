@@ -276,13 +276,19 @@ def run_gpu(args) -> None:
     host = G.TraceResults(WIDTH * HEIGHT, None, host=True)
     e2e_steps = max(1, min(args.steps, 2))
     pipe.trace_host([scene], [cam])  # warm the workspace
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         sa, ca = pipe._arrays([scene], [cam])
         rs = host.struct()
         N.check(N.lib().glc_trace_host(pipe._h, sa, 1, ca, 1, rs), "glc_trace_host")
     e2e_ms = 1e3 * (time.perf_counter() - t0) / e2e_steps
-    e2e = {"value": rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+    if dist:
+        from gravlume_b200.shard import max_over_ranks
+
+        e2e_ms = max_over_ranks(e2e_ms)  # every rank traces its own frame; the slowest sets the pace
+    e2e = {"value": world * rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
            "h2d_bytes_per_step": int(ctypes_sizeof_job()),
            "d2h_bytes_per_step": int(WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
 
