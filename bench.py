@@ -289,8 +289,8 @@ def run_gpu(args) -> None:
 
         e2e_ms = max_over_ranks(e2e_ms)  # every rank traces its own frame; the slowest sets the pace
     e2e = {"value": world * rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
-           "h2d_bytes_per_step": int(ctypes_sizeof_job()),
-           "d2h_bytes_per_step": int(WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
+           "h2d_bytes_per_step": int(world * ctypes_sizeof_job()),
+           "d2h_bytes_per_step": int(world * WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
 
     if rank != 0:
         if dist:
