@@ -252,7 +252,8 @@ GLC_HD C dp5_attempt_compact(const KN<C>& k, const S y0[6], C E, C h, const C k1
 // faster in binary64) or follows the loop as its own call (measured faster in binary32).
 template <class C, class S, bool kInv = true, bool kFold = std::is_same<C, double>::value>
 GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start, const Tolerance& tol,
-                            C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite) {
+                            C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite,
+                            bool track = true) {
   using Coef = StreamCoef<C>;
   C y0c[6];
 #pragma unroll
@@ -279,7 +280,7 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
       }
     }
     if constexpr (kFold) {
-      kn_rhs<C, kInv>(k, ys, E, d, rr, vv, j == 6 ? &inv : nullptr);
+      kn_rhs<C, kInv>(k, ys, E, d, rr, vv, (track && j == 6) ? &inv : nullptr);
     } else {
       kn_rhs<C, false>(k, ys, E, d, rr, vv);
     }
@@ -298,7 +299,7 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
       inc[c] = h * P[0][c];
       ys[c] = y0c[c] + inc[c];
     }
-    kn_rhs<C, kInv>(k, ys, E, d, rr, vv, &inv);
+    kn_rhs<C, kInv>(k, ys, E, d, rr, vv, track ? &inv : nullptr);
 #pragma unroll
     for (int c = 0; c < 7; ++c) err[c] += Coef::e(6) * d[c];
   }
@@ -308,7 +309,7 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
   vr_end = vv;
   dt = h * bt;
   C chk = dt + r_end;
-  if (kInv) chk += inv.lz + inv.carter;
+  if (kInv && track) chk += inv.lz + inv.carter;
   C num = C(0), den = C(1);
 #pragma unroll
   for (int c = 0; c < 7; ++c) {

@@ -373,7 +373,8 @@ __device__ __forceinline__ void trace_one(const JobView& job, const glc_policy& 
     else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
     return;
   }
-  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
+  // the drift maxima are evaluated only when a drift array is wanted
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
   Ray<P> ray;
   ray.init(ls, pol, st8, dir);
   RayResult<S> res;
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
               if (shortcut == kShortCertified) write_certified(out, slot);
               else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
             } else {
-              ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
+              ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
               ray.init(ls, pol, st8, dir);
               active = true;
             }

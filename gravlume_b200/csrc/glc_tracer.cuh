@@ -94,10 +94,14 @@ struct LaneScene {
   // the packed scene, for the surface-transport constants: the result writer reads them after
   // the stepping loop, so that they do not occupy registers through it
   const glc_scene* src;
+  // evaluate L_z, Carter's constant and the null residual at every accepted step for the drift
+  // maxima; off when no drift output is wanted (they do not steer the integration)
+  bool track;
 };
 
-GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor) {
+GLC_HD LaneScene make_lane_scene(const glc_scene& s, double shell_factor, bool track = true) {
   LaneScene ls;
+  ls.track = track;
   ls.kn.a = s.spin;
   ls.kn.a2 = s.spin * s.spin;
   ls.kn.s = s.chart_sign;
@@ -557,12 +561,12 @@ struct Ray {
                                              o.inv, finite);
 #elif GLC_ATTEMPT_FORM == 2
       o.en = dp5_attempt_stream<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
-                                            o.inv, finite);
+                                            o.inv, finite, sc.track);
 #else
       o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
                                      finite);
 #endif
-      if (pair) pair_invariants_after(o);
+      if (pair && sc.track) pair_invariants_after(o);
     }
     if (!finite || !g_finite(o.en)) {
       finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
@@ -631,7 +635,7 @@ struct Ray {
       ah += h;
     }
     commit_azimuth(S(x_old), S(y_old), S(yh[0]), S(yh[1]));
-    update_drifts(o.inv);
+    if (sc.track) update_drifts(o.inv);
     for (int c = 0; c < 7; ++c) k1[c] = o.k7[c];
     r = o.r_end;
     vr = o.vr_end;
@@ -797,7 +801,7 @@ struct Ray {
     {
       int gs;
       const T rr = kn_radius(kt, ycommit[0], ycommit[1], ycommit[2], gs);
-      if (gs == kGeomOk) update_drifts(kn_invariants(kt, ycommit, E, rr));
+      if (sc.track && gs == kGeomOk) update_drifts(kn_invariants(kt, ycommit, E, rr));
     }
     add_affine_s(hh * term_theta);
     set_state(ycommit);
