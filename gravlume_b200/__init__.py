@@ -6,7 +6,7 @@ adaptive Dormand-Prince 5(4) stepper in FP32, MIXED or FP64 precision. This pack
 host binding over that C ABI.
 """
 
-from ._native import GlcError, lib  # noqa: F401
+from ._native import RESULT_FIELDS, GlcError, lib  # noqa: F401
 from .build import LIB_PATH, build  # noqa: F401
 from .trace import (  # noqa: F401
     EquatorialSurface, FootprintStatus, Graph, KerrSchildChart, Observation, Precision, ReferencePolicy, Termination,
