@@ -21,8 +21,14 @@ SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_adjoint.cu", "glc_scene.c
 HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh", "glc_escape_map.cuh", "glc_shadow.cuh", "glc_footprint.cuh",
            "glc_dual.cuh", "glc_adjoint.cuh", "glc_radiation.cuh", "glc_internal.h", "glc_context.h"]
 
+# -prec-div=false / -prec-sqrt=false: binary32 division and square root by the approximate
+# hardware sequences (a couple of ulp) rather than the correctly rounded ones, which the binary32
+# stepping loop executes on every right-hand side (FP32 about 1.35x faster). Binary64 arithmetic
+# and the directed-rounding intrinsics of the capture certificates are not affected; denormals are
+# kept (no -ftz), so the certificates' upward-rounded bounds stay sound.
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+    "-prec-div=false", "-prec-sqrt=false",
     "-Xcompiler", "-fPIC", "-shared",
 ]
 
