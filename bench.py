@@ -37,7 +37,7 @@ L2_BYTES = 126 * 2 ** 20
 # scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32,fp64}_1280x720_full.md): the result
 # stores (200 B/ray, part of which the 126 MB L2 still holds when a 720p launch ends), scaled by the
 # ray count.
-TRAFFIC_BYTES_PER_RAY = {"mixed": (1.748736e6 + 141.551104e6) / 921600, "fp32": (2.924544e6 + 143.304704e6) / 921600,
+TRAFFIC_BYTES_PER_RAY = {"mixed": (3.697920e6 + 139.899904e6) / 921600, "fp32": (3.149056e6 + 146.922240e6) / 921600,
                          "fp64": (8.472576e6 + 141.483776e6) / 921600}
 
 
