@@ -16,6 +16,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB_PATH = LIB_DIR / "libglc.so"
+# the nvcc flags and sources the library was last built with; a change of either rebuilds it
+STAMP_PATH = LIB_DIR / "libglc.build"
 
 SOURCES = ["glc_api.cu", "glc_static_scratch.cu", "glc_adjoint.cu", "glc_scene.cpp", "glc_flops.cpp"]
 HEADERS = ["glc_geometry.cuh", "glc_dp54.cuh", "glc_tracer.cuh", "glc_kernels.cuh", "glc_certificate.cuh", "glc_escape_map.cuh", "glc_shadow.cuh", "glc_footprint.cuh",
@@ -40,8 +42,14 @@ def nvcc() -> str:
     return cand
 
 
+def _stamp() -> str:
+    return " ".join(NVCC_FLAGS + SOURCES)
+
+
 def _stale() -> bool:
     if not LIB_PATH.exists():
+        return True
+    if not STAMP_PATH.exists() or STAMP_PATH.read_text() != _stamp():
         return True
     t = LIB_PATH.stat().st_mtime
     deps = [CSRC / s for s in SOURCES + HEADERS] + [ROOT / "include" / "glc.h"]
@@ -57,6 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
            *[str(CSRC / s) for s in SOURCES], "-lcudart"]
     subprocess.run(cmd, check=True, cwd=str(CSRC))
     os.replace(tmp, LIB_PATH)
+    STAMP_PATH.write_text(_stamp())
     return LIB_PATH
 
 

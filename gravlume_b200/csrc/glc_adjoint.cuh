@@ -48,17 +48,7 @@ GLC_HD KN<D9> kn_dual(const KN<double>& k) {
 // Stage-matrix row i (0-based stage), coefficient of stage j < i; row 6 holds the fifth-order
 // weights (stage 7's point is the end state). The device reads the constant-memory table (a local
 // array indexed at run time would be rebuilt in local memory on every call).
-GLC_HD double dp_coef(int i, int j) {
-#if defined(__CUDA_ARCH__)
-  return kDpA[i][j];
-#else
-  using namespace dp;
-  const double A[7][6] = {{0, 0, 0, 0, 0, 0},         {a21, 0, 0, 0, 0, 0},         {a31, a32, 0, 0, 0, 0},
-                          {a41, a42, a43, 0, 0, 0},   {a51, a52, a53, a54, 0, 0},   {a61, a62, a63, a64, a65, 0},
-                          {b1, 0, b3, b4, b5, b6}};
-  return A[i][j];
-#endif
-}
+GLC_HD double dp_coef(int i, int j) { return dp_a<double>(i, j); }
 
 // Weights of the fifth-order end point (stage 7 unused).
 GLC_HD void step_weights(double w[7]) {

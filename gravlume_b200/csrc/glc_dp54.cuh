@@ -39,49 +39,19 @@ constexpr double d71 = 40617522.0 / 29380423.0, d72 = -110615467.0 / 29380423.0,
 
 // Stage matrix as a table for the compact attempt (row s: coefficients of stages 0..s-1; row 6 is
 // the fifth-order weights, so stage 7's point is the end state), and the error weights b - b*.
-#if defined(__CUDACC__)
-__constant__ double kDpA[7][6] = {
-#else
-static const double kDpA[7][6] = {
-#endif
-    {0, 0, 0, 0, 0, 0},
-    {dp::a21, 0, 0, 0, 0, 0},
-    {dp::a31, dp::a32, 0, 0, 0, 0},
-    {dp::a41, dp::a42, dp::a43, 0, 0, 0},
-    {dp::a51, dp::a52, dp::a53, dp::a54, 0, 0},
-    {dp::a61, dp::a62, dp::a63, dp::a64, dp::a65, 0},
-    {dp::b1, 0, dp::b3, dp::b4, dp::b5, dp::b6},
-};
-#if defined(__CUDACC__)
-__constant__ float kDpAf[7][6] = {
-#else
-static const float kDpAf[7][6] = {
-#endif
-    {0, 0, 0, 0, 0, 0},
-    {float(dp::a21), 0, 0, 0, 0, 0},
-    {float(dp::a31), float(dp::a32), 0, 0, 0, 0},
-    {float(dp::a41), float(dp::a42), float(dp::a43), 0, 0, 0},
-    {float(dp::a51), float(dp::a52), float(dp::a53), float(dp::a54), 0, 0},
-    {float(dp::a61), float(dp::a62), float(dp::a63), float(dp::a64), float(dp::a65), 0},
-    {float(dp::b1), 0, float(dp::b3), float(dp::b4), float(dp::b5), float(dp::b6)},
-};
-
-template <class T>
-GLC_HD T dp_a(int s, int j);
-template <>
-GLC_HD float dp_a<float>(int s, int j) { return kDpAf[s][j]; }
-template <>
-GLC_HD double dp_a<double>(int s, int j) { return kDpA[s][j]; }
+#define GLC_DP_A(T)                                                                                   \
+  {{T(0), T(0), T(0), T(0), T(0), T(0)},                                                              \
+   {T(dp::a21), T(0), T(0), T(0), T(0), T(0)},                                                        \
+   {T(dp::a31), T(dp::a32), T(0), T(0), T(0), T(0)},                                                  \
+   {T(dp::a41), T(dp::a42), T(dp::a43), T(0), T(0), T(0)},                                            \
+   {T(dp::a51), T(dp::a52), T(dp::a53), T(dp::a54), T(0), T(0)},                                      \
+   {T(dp::a61), T(dp::a62), T(dp::a63), T(dp::a64), T(dp::a65), T(0)},                                \
+   {T(dp::b1), T(0), T(dp::b3), T(dp::b4), T(dp::b5), T(dp::b6)}}
 
 // Streaming form of the stage matrix: after the slope of stage j (0-based) is known it is added,
 // with weight kStreamA[j][m] = A[j+1+m][j], into the pending point sum of stage j+1+m; the sums
 // rotate so that the next stage's sum is always first (row 6, after the end-point slope, is zero).
 // kStreamE / kStreamB are the error weights b - b* and the fifth-order weights b per stage.
-#if defined(__CUDACC__)
-#define GLC_TABLE __constant__
-#else
-#define GLC_TABLE static const
-#endif
 #define GLC_STREAM_A(T)                                                                                  \
   {{T(dp::a21), T(dp::a31), T(dp::a41), T(dp::a51), T(dp::a61), T(dp::b1)},                             \
    {T(dp::a32), T(dp::a42), T(dp::a52), T(dp::a62), T(0), T(0)},                                         \
@@ -92,31 +62,60 @@ GLC_HD double dp_a<double>(int s, int j) { return kDpA[s][j]; }
    {T(0), T(0), T(0), T(0), T(0), T(0)}}
 #define GLC_STREAM_E(T) {T(dp::e1), T(0), T(dp::e3), T(dp::e4), T(dp::e5), T(dp::e6), T(dp::e7)}
 #define GLC_STREAM_B(T) {T(dp::b1), T(0), T(dp::b3), T(dp::b4), T(dp::b5), T(dp::b6), T(0)}
-GLC_TABLE float kStreamAf[7][6] = GLC_STREAM_A(float);
-GLC_TABLE double kStreamAd[7][6] = GLC_STREAM_A(double);
-GLC_TABLE float kStreamEf[7] = GLC_STREAM_E(float);
-GLC_TABLE double kStreamEd[7] = GLC_STREAM_E(double);
-GLC_TABLE float kStreamBf[7] = GLC_STREAM_B(float);
-GLC_TABLE double kStreamBd[7] = GLC_STREAM_B(double);
+
+// The device reads constant memory at a warp-uniform index; host code (the host builds of these
+// templates, and the host pass of nvcc) reads ordinary static copies of the same tables.
+#if defined(__CUDACC__)
+__constant__ double kDpA[7][6] = GLC_DP_A(double);
+__constant__ float kDpAf[7][6] = GLC_DP_A(float);
+__constant__ float kStreamAf[7][6] = GLC_STREAM_A(float);
+__constant__ double kStreamAd[7][6] = GLC_STREAM_A(double);
+__constant__ float kStreamEf[7] = GLC_STREAM_E(float);
+__constant__ double kStreamEd[7] = GLC_STREAM_E(double);
+__constant__ float kStreamBf[7] = GLC_STREAM_B(float);
+__constant__ double kStreamBd[7] = GLC_STREAM_B(double);
+#endif
+static const double kDpAHost[7][6] = GLC_DP_A(double);
+static const float kDpAfHost[7][6] = GLC_DP_A(float);
+static const float kStreamAfHost[7][6] = GLC_STREAM_A(float);
+static const double kStreamAdHost[7][6] = GLC_STREAM_A(double);
+static const float kStreamEfHost[7] = GLC_STREAM_E(float);
+static const double kStreamEdHost[7] = GLC_STREAM_E(double);
+static const float kStreamBfHost[7] = GLC_STREAM_B(float);
+static const double kStreamBdHost[7] = GLC_STREAM_B(double);
+#undef GLC_DP_A
 #undef GLC_STREAM_A
 #undef GLC_STREAM_E
 #undef GLC_STREAM_B
-#undef GLC_TABLE
+
+#if defined(__CUDA_ARCH__)
+#define GLC_COEF(table) table
+#else
+#define GLC_COEF(table) table##Host
+#endif
+
+template <class T>
+GLC_HD T dp_a(int s, int j);
+template <>
+GLC_HD float dp_a<float>(int s, int j) { return GLC_COEF(kDpAf)[s][j]; }
+template <>
+GLC_HD double dp_a<double>(int s, int j) { return GLC_COEF(kDpA)[s][j]; }
 
 template <class T>
 struct StreamCoef;
 template <>
 struct StreamCoef<float> {
-  static GLC_HD float a(int j, int m) { return kStreamAf[j][m]; }
-  static GLC_HD float e(int j) { return kStreamEf[j]; }
-  static GLC_HD float b(int j) { return kStreamBf[j]; }
+  static GLC_HD float a(int j, int m) { return GLC_COEF(kStreamAf)[j][m]; }
+  static GLC_HD float e(int j) { return GLC_COEF(kStreamEf)[j]; }
+  static GLC_HD float b(int j) { return GLC_COEF(kStreamBf)[j]; }
 };
 template <>
 struct StreamCoef<double> {
-  static GLC_HD double a(int j, int m) { return kStreamAd[j][m]; }
-  static GLC_HD double e(int j) { return kStreamEd[j]; }
-  static GLC_HD double b(int j) { return kStreamBd[j]; }
+  static GLC_HD double a(int j, int m) { return GLC_COEF(kStreamAd)[j][m]; }
+  static GLC_HD double e(int j) { return GLC_COEF(kStreamEd)[j]; }
+  static GLC_HD double b(int j) { return GLC_COEF(kStreamBd)[j]; }
 };
+#undef GLC_COEF
 
 struct Tolerance {
   double pos_rtol, pos_atol, mom_rtol, mom_atol;

@@ -37,6 +37,22 @@ def test_library_exports_every_declared_symbol():
     assert lib.glc_status_string(0) == b"ok"
 
 
+def test_build_flags_keep_the_capture_certificates_sound():
+    """sm_100a only; binary32 division and square root may be approximate, but nothing may flush
+    denormals or turn on fast math: the certificates' directed-rounding bounds rely on both."""
+    import importlib
+
+    flags = importlib.import_module("gravlume_b200.build").NVCC_FLAGS
+    assert "arch=compute_100a,code=sm_100a" in flags
+    assert "-prec-div=false" in flags and "-prec-sqrt=false" in flags
+    for bad in ("-ftz=true", "--ftz=true", "-use_fast_math", "--use_fast_math"):
+        assert bad not in flags, bad
+    cert = (ROOT / "gravlume_b200" / "csrc" / "glc_certificate.cuh").read_text()
+    for rounded in ("__fadd_rd", "__fadd_ru", "__fmul_rd", "__fmul_ru", "__fdiv_rd", "__fdiv_ru",
+                    "__fsqrt_rd", "__fsqrt_ru"):
+        assert rounded in cert, rounded
+
+
 def test_create_without_a_device_is_a_typed_error():
     import torch
 
