@@ -136,8 +136,8 @@ def sample_pixels(n: int, seed: int = 64):
     return idx % WIDTH, idx // WIDTH, idx
 
 
-def cpu_oracle_sample(G, n_rays: int, threads: int):
-    """Binary64 oracle (rtol 1e-10, atol 1e-12) on a seeded pixel sample of the frame."""
+def oracle_job(G):
+    """The headline frame as the CPU oracle's scene and events."""
     import oracle as O
 
     obs = make_observation(G)
@@ -145,11 +145,53 @@ def cpu_oracle_sample(G, n_rays: int, threads: int):
                   height=HEIGHT, vertical_fov=obs.vertical_fov)
     ev = O.events(escape_radius=ESCAPE, surface=(obs.surface.inner_radius, SURFACE_OUTER),
                   horizon_offset=HORIZON_OFFSET)
+    return osc, ev
+
+
+def cpu_oracle_sample(G, n_rays: int, threads: int):
+    """Binary64 oracle (rtol 1e-10, atol 1e-12) on a seeded pixel sample of the frame."""
+    import oracle as O
+
+    osc, ev = oracle_job(G)
     px, py, idx = sample_pixels(n_rays)
     t0 = time.perf_counter()
     ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
     dt = time.perf_counter() - t0
     return ref, idx, dt
+
+
+def reference_gpu_algorithm_report(G, ref, idx, threads: int) -> dict:
+    """Errors of the reference's own GPU algorithm (binary32 fixed-policy RK4, restated on the CPU
+    as the second comparator) on the same oracle sample, for comparison with the CUDA modes."""
+    import numpy as np
+    import oracle as O
+
+    osc, ev = oracle_job(G)
+    t0 = time.perf_counter()
+    rows = O.rk4_pixels(osc, ev, idx % WIDTH, idx // WIDTH, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    F, R = O.F, O.RK4
+    rt = rows[:, R["termination"]].astype(int)
+    ot = ref[:, F["termination"]].astype(int)
+    same = rt == ot
+    rep = {"algorithm": "binary32 RK4, h = clamp(0.1 r, 0.005, 8), at most 2048 steps (geodesic_integration.wgsl)",
+           "rays": int(idx.size), "class_mismatch": int((~same).sum()),
+           "uncertain": int((rt == O.UNCERTAIN).sum()), "step_exhaustion": int((rt == O.STEP_EXHAUSTION).sum()),
+           "steps_mean": float(rows[:, R["steps"]].mean()),
+           "cpu_mrays_per_s": idx.size / cpu_s / 1e6, "cores": threads}
+    esc = same & (ot == O.ESCAPE)
+    if esc.any():
+        d = np.stack([ref[esc, F["escape_dx"]], ref[esc, F["escape_dy"]], ref[esc, F["escape_dz"]]], axis=1)
+        v = rows[esc][:, [R["source0"], R["source1"], R["source2"]]]
+        rep["escape_direction_rad"] = float(np.max(np.arccos(np.clip((d * v).sum(1), -1, 1))))
+    srf = same & (ot == O.SURFACE)
+    if srf.any():
+        g0 = ref[srf, F["frequency_ratio"]]
+        rep["g_rel"] = float(np.max(np.abs(rows[srf, R["source2"]] - g0) / g0))
+        rep["hit_radius"] = float(np.max(np.abs(rows[srf, R["source0"]] - ref[srf, F["source_radius"]])))
+    if same.any():
+        rep["travel_time"] = float(np.max(np.abs(rows[same, R["travel_time"]] - ref[same, F["travel_time"]])))
+    return rep
 
 
 def run_reference(args) -> None:
@@ -353,6 +395,7 @@ def run_gpu(args) -> None:
                                     "sample": f"{args.cpu_sample} seeded pixels of the {WIDTH}x{HEIGHT} frame, "
                                               "binary64 oracle rtol 1e-10 atol 1e-12"}
             comp[args.precision] = error_report(G, d, ref, idx)
+            comp["reference_gpu_algorithm"] = reference_gpu_algorithm_report(G, ref, idx, threads)
         shape = {k: policy[k] for k in ("persistent", "block_threads", "tile_w", "tile_h", "refill_interval",
                                          "rays_per_grab")}
         frame_tol = {k: policy[k] for k in ("position_rtol", "position_atol", "momentum_rtol", "momentum_atol",

@@ -84,9 +84,17 @@ class ObserverInfo(ctypes.Structure):
     ]
 
 
+def _stale() -> bool:
+    if not LIB_PATH.exists():
+        return True
+    t = LIB_PATH.stat().st_mtime
+    sources = list(_HERE.glob("*.hpp")) + list(_HERE.glob("*.cpp")) + [_HERE / "Makefile"]
+    return any(p.stat().st_mtime > t for p in sources)
+
+
 def build(force: bool = False) -> Path:
     """Compile the oracle with its Makefile (gcc only; no GPU needed)."""
-    if force or not LIB_PATH.exists():
+    if force or _stale():
         subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
     return LIB_PATH
 
@@ -97,8 +105,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            build()
+        build()
         L = ctypes.CDLL(str(LIB_PATH))
         dp = ctypes.POINTER(ctypes.c_double)
         L.gro_fields.restype = ctypes.c_int
@@ -262,6 +269,34 @@ def trace_pixels(sc: Scene, policy, ev, px, py, sx=0.5, sy=0.5, threads=1):
     if rc != 0:
         raise ValueError(f"trace configuration rejected ({rc})")
     return out, status
+
+
+# Row layout of rk4_pixels (the reference's binary32 GPU RK4 kernel, restated).
+RK4_FIELDS = ["termination", "flags", "event_candidates", "steps", "event_residual", "source0", "source1",
+              "source2", "travel_time", "null_residual", "energy_drift", "lz_drift", "carter_drift",
+              "radial_turnings", "equatorial_crossings", "azimuth_winding"]
+RK4 = {name: i for i, name in enumerate(RK4_FIELDS)}
+
+
+def rk4_pixels(sc: Scene, ev, px, py, sx=0.5, sy=0.5, threads=1):
+    """The reference's own GPU algorithm (geodesic_integration.wgsl: binary32 classical RK4 with
+    h = clamp(0.1 r, 0.005, 8), at most 2048 steps, Hermite event localization) on image samples;
+    a second comparator beside the binary64 oracle. Escape rows hold the unit escape direction in
+    source0..2; surface rows hold (radius, azimuth, g)."""
+    L = lib()
+    L.gro_rk4_pixels.argtypes = [ctypes.POINTER(Scene), ctypes.POINTER(Events), ctypes.c_int64] + [
+        ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_void_p]
+    px = _c(px, np.uint32)
+    n = px.size
+    py = _c(py, np.uint32)
+    sx = _c(np.broadcast_to(sx, (n,)), np.float64)
+    sy = _c(np.broadcast_to(sy, (n,)), np.float64)
+    out = np.full((n, len(RK4_FIELDS)), np.nan)
+    rc = L.gro_rk4_pixels(ctypes.byref(sc), ctypes.byref(ev), n, px.ctypes.data, py.ctypes.data,
+                          sx.ctypes.data, sy.ctypes.data, threads, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"trace configuration rejected ({rc})")
+    return out
 
 
 def surface_observable(mass, spin, charge, chart, inner, outer, state, observer_frequency=1.0,

@@ -14,6 +14,7 @@
 #include "oracle_footprint.hpp"
 #include "oracle_radiation.hpp"
 #include "oracle_tracer.hpp"
+#include "oracle_wgsl_rk4.hpp"
 
 using namespace gro;
 
@@ -440,6 +441,73 @@ int gro_ind_gradients(double m, double a, double q, int chart, const gro_policy*
       }
     }
     row[1] = 1.0;
+  });
+  return 0;
+}
+
+// The reference's GPU RK4 kernel restated in binary32 (oracle_wgsl_rk4.hpp) over image samples,
+// with the uniforms input.rs:64-131 packs: M = 1, the chart as +1 ingoing / -1 outgoing, the tetrad
+// legs and tan(fov/2) narrowed from binary64, guard 2^-40, tie tolerance 2^-17 M, arming band
+// 2^-12 M, step policy (0.1, 0.005, 8) and drift limit 0.05. The event surfaces are the job's
+// (escape radius; capture at the outer horizon of the narrowed spacetime plus the job's offset;
+// surface radii). out: 16 doubles per ray = termination, failure flags, event candidates, steps,
+// event residual, source[3] (escape: unit -dx/dlambda; surface: radius, azimuth, g), travel time,
+// drift[4] (null residual, 0, L_z, Carter), radial turnings, equatorial crossings, azimuth winding.
+int gro_rk4_pixels(const gro_scene* s, const gro_events* ev, int64_t n, const uint32_t* px, const uint32_t* py,
+                   const double* sx, const double* sy, int threads, double* out) {
+  Spacetime sp;
+  StationaryObserver obs;
+  PerspectiveView view;
+  const int rc = build_scene(*s, sp, obs, view);
+  if (rc != 0) return rc;
+  if (bits_of(sp.mass_m) != bits_of(1.0)) return -2;
+  if (!ev->has_escape) return -5;
+  rk4::Uniforms U{};
+  U.mass = 1.0f;
+  U.spin = float(s->spin);
+  U.charge = float(s->charge);
+  U.chart = s->chart ? -1.0f : 1.0f;
+  U.observer = {float(obs.event[1]), float(obs.event[2]), float(obs.event[3])};
+  for (int i = 0; i < 4; ++i) {
+    U.velocity[i] = float(obs.frame.four_velocity.v[i]);
+    U.right[i] = float(obs.frame.image_right.v[i]);
+    U.up[i] = float(obs.frame.image_up.v[i]);
+    U.arrival[i] = float(obs.frame.arrival.v[i]);
+  }
+  U.tan_half_fov = float(view.tangent_half_fov);
+  U.frequency = 1.0f;
+  Spacetime narrowed;
+  double rp = -1.0;
+  if (Spacetime::make(1.0, double(U.spin), double(U.charge), sp.chart, narrowed) && narrowed.outer_horizon_radius(rp))
+    rp += ev->horizon_offset;
+  else
+    rp = -1.0;
+  U.escape = float(ev->escape_radius);
+  U.guard = 0x1p-40f;
+  U.horizon = float(rp);
+  U.tie = 0x1p-17f;
+  U.surface = ev->has_surface != 0;
+  U.inner = U.surface ? float(ev->surface_inner) : 0.0f;
+  U.outer = U.surface ? float(ev->surface_outer) : 0.0f;
+  U.arming = U.surface ? 0x1p-12f : 0.0f;
+  U.step_scale = 0.1f;
+  U.step_min = 0.005f;
+  U.step_max = 8.0f;
+  U.drift_limit = 0.05f;
+  parallel_for(n, threads, [&](int64_t i) {
+    const rk4::Result r = rk4::trace_pixel(U, s->width, s->height, px[i], py[i], float(sx[i]), float(sy[i]));
+    double* row = out + 16 * i;
+    row[0] = r.termination;
+    row[1] = r.flags;
+    row[2] = r.candidates;
+    row[3] = r.steps;
+    row[4] = r.event_residual;
+    for (int k = 0; k < 3; ++k) row[5 + k] = r.source[k];
+    row[8] = r.travel_time;
+    for (int k = 0; k < 4; ++k) row[9 + k] = r.drift[k];
+    row[13] = r.turnings;
+    row[14] = r.crossings;
+    row[15] = r.winding;
   });
   return 0;
 }

@@ -1,4 +1,5 @@
-"""Regenerate tests/golden/reference_fixtures.json from the reference's versioned TOML fixtures.
+"""Regenerate tests/golden/reference_fixtures.json from the reference's versioned TOML fixtures,
+and tests/golden/gpu_gate_cases.json from the reference's GPU-against-CPU tests.
 
 The reference pins its CPU oracle with strict TOML known-answer fixtures
 (crates/gravlume-reference/fixtures/v1/*.toml and fixtures/v2/kerr-surface-observable.toml,
@@ -65,6 +66,68 @@ def radiation_known_answers(reference_root: str) -> dict:
     return out
 
 
+# The reference's GPU-against-CPU gates (crates/gravlume-render/src/gpu_trace_tests.rs and
+# gpu_trace_tests/surface.rs): the image samples, scenes and tolerances they check the WGSL RK4
+# kernel with. The scene helpers are restated here, cited; the sample tables and tolerances are
+# read from the test source.
+_ANGLES = {"FRAC_PI_2": "pi/2", "FRAC_PI_3": "pi/3", "FRAC_PI_4": "pi/4"}
+
+
+def gpu_gate_cases(reference_root: str) -> dict:
+    import re
+
+    root = Path(reference_root) / "crates" / "gravlume-render" / "src"
+    rel = "crates/gravlume-render/src/gpu_trace_tests.rs"
+    src = (root / "gpu_trace_tests.rs").read_text()
+    test = "headless_gpu_regular_matrix_matches_reference_termination_and_escape_direction"
+    body = src[src.index(f"fn {test}()"):]
+    body = body[: body.index("\n}\n")]
+    extent = re.search(r"default_observation\((\d+),\s*(\d+)\)", body)
+    samples = [[int(x), int(y)] for x, y in re.findall(r"sample\(&observation,\s*(\d+),\s*(\d+),", body)]
+    regular = {
+        "_source": f"{rel} ({test}; observation_at_scale, observation_with_time)",
+        "width": int(extent.group(1)), "height": int(extent.group(2)),
+        # observation_at_scale (mass 1): a = 0.8 M, Q = 0, outgoing chart, observer at oblate
+        # (30 M, pi/3, 0) looking at the origin with +z up, omega = 1, vertical FOV pi/4; the
+        # CPU side traces ObservationTracer::baseline_v1 (escape at 200 M) with regular_v1.
+        "spin": 0.8, "charge": 0.0, "chart": "outgoing", "observer_oblate": [30.0, "pi/3", 0.0],
+        "vertical_fov": "pi/4", "escape_radius": 200.0,
+        "samples": samples,
+        "escape_angle_rad": float(re.search(r"angular_error <= ([0-9.e-]+)", body).group(1)),
+        "event_residual": float(re.search(r"event_residual <= ([0-9.e-]+)", body).group(1)),
+        "travel_time_m": float(re.search(r"travel_time_error <= ([0-9.e-]+)", body).group(1)),
+        "drift_limit": 0.05,  # INVARIANT_DRIFT_LIMIT (crates/gravlume-render/src/trace/input.rs:13)
+    }
+    rel_s = "crates/gravlume-render/src/gpu_trace_tests/surface.rs"
+    ssrc = (root / "gpu_trace_tests" / "surface.rs").read_text()
+    table = ssrc[ssrc.index("const SURFACE_BRANCH_PROFILES"):]
+    table = table[: table.index("\n];\n")]
+    profiles = []
+    for block in table.split("SurfaceBranchProfile {")[1:]:
+        fov = re.search(r"vertical_fov: std::f64::consts::(\w+)", block).group(1)
+        profiles.append({
+            "label": re.search(r'label: "([^"]+)"', block).group(1),
+            "spin": float(re.search(r"spin: ([-0-9.]+)", block).group(1)),
+            "charge": float(re.search(r"charge: ([-0-9.]+)", block).group(1)),
+            "observer_radius": float(re.search(r"observer_radius: ([0-9.]+)", block).group(1)),
+            "vertical_fov": _ANGLES[fov],
+            "samples": [[int(x), int(y)] for x, y in re.findall(r"\((\d+),\s*(\d+)\)", block)],
+        })
+    fn = ssrc[ssrc.index("fn assert_surface_branch_profile"):]
+    ext = re.search(r"vertical_fov,\s*(\d+),\s*(\d+),", fn)
+    emit = re.search(r"inverse_cube_bolometric_v1\(([0-9.]+),\s*([0-9.]+),", fn)
+    surface = {
+        "_source": f"{rel_s} (gpu_surface_branches_match_fixed_reference_samples); "
+                   f"{rel} (transfer_profile_extent)",
+        # transfer_profile_extent: outgoing chart, observer at oblate (r, pi/3, 0) looking at the
+        # origin with +z up, omega = 1; vacuum inverse-cube bolometric surface; escape at 200 M.
+        "width": int(ext.group(1)), "height": int(ext.group(2)), "observer_polar": "pi/3",
+        "surface": [float(emit.group(1)), float(emit.group(2))], "escape_radius": 200.0,
+        "profiles": profiles,
+    }
+    return {"regular_matrix": regular, "surface_branches": surface}
+
+
 def main(reference_root: str) -> None:
     base = Path(reference_root) / "crates" / "gravlume-reference" / "fixtures"
     out = {}
@@ -76,6 +139,9 @@ def main(reference_root: str) -> None:
     target = Path(__file__).with_name("reference_fixtures.json")
     target.write_text(json.dumps(out, indent=1, sort_keys=True) + "\n")
     print(f"wrote {target} ({len(out)} fixtures)")
+    gates = Path(__file__).with_name("gpu_gate_cases.json")
+    gates.write_text(json.dumps(gpu_gate_cases(reference_root), indent=1) + "\n")
+    print(f"wrote {gates}")
 
 
 if __name__ == "__main__":
