@@ -6,6 +6,12 @@
  * land in caller-owned device arrays. Nothing here aborts the process: every failure is a
  * glc_status, and glc_last_error_string() describes the last one on the calling thread.
  *
+ * Threading: a glc_ctx holds its own staging buffers, streams and grow-only workspaces and takes
+ * no lock, so one context serves one host thread at a time (the reference drives one wgpu queue
+ * per pipeline the same way). Use one context per host thread, or serialize the calls on a shared
+ * one. Contexts on the same device are independent; the host-only helpers (glc_scene_pack,
+ * glc_policy_default, glc_result_slots, ...) are thread-safe.
+ *
  * The entry points replace the reference's trace boundary (paths are within romeoahmed/gravlume):
  *   glc_scene_pack   <- TraceUniforms::from_observation_with_surface
  *                       (crates/gravlume-render/src/trace/input.rs:45-131), with the domain
