@@ -318,6 +318,18 @@ def invariants(mass, spin, charge, chart, state):
     return out
 
 
+def metric_covariant(mass, spin, charge, chart, txyz):
+    """g_{mu nu} at a Cartesian Kerr-Schild event (4x4), or None where the geometry is singular."""
+    L = lib()
+    L.gro_metric_covariant.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    ev = _c(txyz, np.float64)
+    out = np.zeros(16)
+    rc = L.gro_metric_covariant(mass, spin, charge, chart, ev.ctypes.data, out.ctypes.data)
+    if rc == -1:
+        raise ValueError("invalid spacetime parameters")
+    return None if rc != 0 else out.reshape(4, 4)
+
+
 def hamiltonian_rhs(mass, spin, charge, chart, state):
     st = _c(state, np.float64)
     out = np.zeros(8)

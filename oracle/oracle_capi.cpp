@@ -445,6 +445,21 @@ int gro_ind_gradients(double m, double a, double q, int chart, const gro_policy*
   return 0;
 }
 
+// KerrNewmanSpacetime::metric_covariant_at (spacetime.rs:485-490): g_{mu nu} = eta + f l l at a
+// Cartesian Kerr-Schild event; out16 row-major. Returns 0, or -1 for invalid parameters and
+// -2 where the geometry is singular.
+int gro_metric_covariant(double m, double a, double q, int chart, const double* txyz, double* out16) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -1;
+  Geometry g;
+  if (sp.geometry(txyz, g) != GeometryError::None) return -2;
+  double mm[4][4];
+  Spacetime::metric_covariant(g, mm);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) out16[4 * r + c] = mm[r][c];
+  return 0;
+}
+
 // The reference's GPU RK4 kernel restated in binary32 (oracle_wgsl_rk4.hpp) over image samples,
 // with the uniforms input.rs:64-131 packs: M = 1, the chart as +1 ingoing / -1 outgoing, the tetrad
 // legs and tan(fov/2) narrowed from binary64, guard 2^-40, tie tolerance 2^-17 M, arming band
