@@ -164,7 +164,7 @@ def lib(path: Path | None = None):
     if _lib is None:
         p = Path(path or LIB_PATH)
         if not p.exists():
-            raise RuntimeError(f"libglc.so is not built ({p}); run gravlume_b200.build.build()")
+            raise RuntimeError(f"libglc.so is not built ({p}); run gravlume_b200.build(force=True)")
         L = ctypes.CDLL(str(p))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)

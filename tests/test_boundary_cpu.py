@@ -37,6 +37,18 @@ def test_library_exports_every_declared_symbol():
     assert lib.glc_status_string(0) == b"ok"
 
 
+def test_a_missing_library_fails_loudly():
+    """No fallback: without libglc.so the bindings raise, naming the build call."""
+    import subprocess
+    import sys
+
+    code = ("from gravlume_b200 import _native as N\n"
+            "try:\n    N.lib('/nonexistent/libglc.so')\nexcept RuntimeError as e:\n    print(e)\n")
+    run = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=str(ROOT), timeout=120)
+    assert run.returncode == 0, run.stderr
+    assert "libglc.so is not built" in run.stdout and "gravlume_b200.build(force=True)" in run.stdout
+
+
 def test_build_flags_keep_the_capture_certificates_sound():
     """sm_100a only; binary32 division and square root may be approximate, but nothing may flush
     denormals or turn on fast math: the certificates' directed-rounding bounds rely on both."""
