@@ -54,6 +54,44 @@ def workload_config(precision: str, policy: dict | None = None) -> dict:
     return cfg
 
 
+def compact_config(precision: str, policy: dict) -> dict:
+    """The headline line's config: the workload and the policy fields that set its cost."""
+    return {"workload": f"kerr-newman-frame-{WIDTH}x{HEIGHT}",
+            "scene": f"a={SPIN} Q={CHARGE} i={INCL_DEG:g}deg r_obs={R_OBS:g}M fov={FOV_DEG:g}deg",
+            "precision": precision, "rtol": policy.get("position_rtol"), "l2": "flushed between frames"}
+
+
+def compact_roofline(r: dict) -> dict:
+    """The headline line's roofline: the dominant kernel's algorithmic FP32 FMA rate against the
+    nominal FP32 FMA peak, the DRAM traffic per launch and the HBM fraction of its result stores."""
+    return {"bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"], "unit": r["unit"], "frac": r["frac"],
+            "traffic": r["traffic"], "peak_source": "nominal",
+            "hbm_frac": r["hbm_view"]["frac"]}
+
+
+def make_headline(value, world, steps, warmup, ms_per_step, precision, policy, launches, clk, e2e, roofline) -> dict:
+    """The last stdout line: the contract keys only, well under 1 KB (the studies go on earlier lines)."""
+    return rounded({
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": steps, "warmup": warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "mixed": "f32+f64", "fp64": "f64"}[precision],
+        "data": "synthetic", "config": compact_config(precision, policy),
+        "gpu_launches": int(launches), "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "e2e": e2e, "roofline": compact_roofline(roofline),
+    })
+
+
+def rounded(x, digits: int = 6):
+    """x with every float rounded to `digits` significant digits (for the short headline line)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}") if math.isfinite(x) else x
+    if isinstance(x, dict):
+        return {k: rounded(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [rounded(v, digits) for v in x]
+    return x
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -136,23 +174,25 @@ def sample_pixels(n: int, seed: int = 64):
     return idx % WIDTH, idx // WIDTH, idx
 
 
-def oracle_job(G):
-    """The headline frame as the CPU oracle's scene and events."""
+def oracle_job():
+    """The headline frame as the CPU oracle's scene and events, set up from the oracle alone (its
+    own observer placement and ISCO), so that a process that only runs the oracle maps no product
+    library. The observer position equals make_observation's to the last bit (a CPU test checks)."""
     import oracle as O
 
-    obs = make_observation(G)
-    osc = O.scene(mass=1.0, spin=SPIN, charge=CHARGE, chart=1, observer_txyz=obs.observer_txyz, width=WIDTH,
-                  height=HEIGHT, vertical_fov=obs.vertical_fov)
-    ev = O.events(escape_radius=ESCAPE, surface=(obs.surface.inner_radius, SURFACE_OUTER),
+    txyz = [0.0, *O.oblate_to_cartesian(SPIN, 1, R_OBS, math.radians(INCL_DEG), 0.0)]
+    osc = O.scene(mass=1.0, spin=SPIN, charge=CHARGE, chart=1, observer_txyz=txyz, width=WIDTH,
+                  height=HEIGHT, vertical_fov=math.radians(FOV_DEG))
+    ev = O.events(escape_radius=ESCAPE, surface=(O.prograde_isco(1.0, SPIN, CHARGE), SURFACE_OUTER),
                   horizon_offset=HORIZON_OFFSET)
     return osc, ev
 
 
-def cpu_oracle_sample(G, n_rays: int, threads: int):
+def cpu_oracle_sample(n_rays: int, threads: int):
     """Binary64 oracle (rtol 1e-10, atol 1e-12) on a seeded pixel sample of the frame."""
     import oracle as O
 
-    osc, ev = oracle_job(G)
+    osc, ev = oracle_job()
     px, py, idx = sample_pixels(n_rays)
     t0 = time.perf_counter()
     ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
@@ -160,13 +200,13 @@ def cpu_oracle_sample(G, n_rays: int, threads: int):
     return ref, idx, dt
 
 
-def reference_gpu_algorithm_report(G, ref, idx, threads: int) -> dict:
+def reference_gpu_algorithm_report(ref, idx, threads: int) -> dict:
     """Errors of the reference's own GPU algorithm (binary32 fixed-policy RK4, restated on the CPU
     as the second comparator) on the same oracle sample, for comparison with the CUDA modes."""
     import numpy as np
     import oracle as O
 
-    osc, ev = oracle_job(G)
+    osc, ev = oracle_job()
     t0 = time.perf_counter()
     rows = O.rk4_pixels(osc, ev, idx % WIDTH, idx // WIDTH, threads=threads)
     cpu_s = time.perf_counter() - t0
@@ -199,16 +239,15 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import gravlume_b200 as G
     import oracle as O
 
     threads = O.hardware_threads()
     n = args.cpu_sample
     times = []
     for _ in range(args.warmup):
-        cpu_oracle_sample(G, max(n // 8, 64), threads)
+        cpu_oracle_sample(max(n // 8, 64), threads)
     for _ in range(args.steps):
-        _, _, dt = cpu_oracle_sample(G, n, threads)
+        _, _, dt = cpu_oracle_sample(n, threads)
         times.append(dt)
     total = sum(times)
     value = n * len(times) / total / 1e6
@@ -224,7 +263,7 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def error_report(G, gpu: dict, ref, idx) -> dict:
+def error_report(gpu: dict, ref, idx) -> dict:
     import numpy as np
     import oracle as O
 
@@ -370,32 +409,29 @@ def run_gpu(args) -> None:
     roofline["hbm_view"] = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
                             "peak_source": f"{hbm_source} copy bandwidth"}
 
-    line = {
-        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": {"fp32": "f32", "mixed": "f32+f64", "fp64": "f64"}[args.precision],
-        "data": "synthetic (camera rays generated on device)", "config": workload_config(args.precision, policy),
-        "gpu_launches": int(launches), "clocks": clk, "e2e": e2e, "roofline": roofline,
-        "class_histogram": np.bincount(d["termination"], minlength=9).tolist(),
-        "steps_per_ray": {"mean": float(d["accepted_steps"].mean()), "max": int(d["accepted_steps"].max()),
-                          "rejected_mean": float(d["rejected_steps"].mean())},
-    }
+    headline = make_headline(value, world, args.steps, args.warmup, total_ms / args.steps, args.precision, policy,
+                             launches, clk, e2e, roofline)
+    studies = {"roofline_detail": roofline, "class_histogram": np.bincount(d["termination"], minlength=9).tolist(),
+               "steps_per_ray": {"mean": float(d["accepted_steps"].mean()), "max": int(d["accepted_steps"].max()),
+                                 "rejected_mean": float(d["rejected_steps"].mean())}}
+
+    # ---- CPU baseline: the binary64 oracle on a bounded seeded sample of the same frame
+    ref = idx = None
+    if args.cpu_sample > 0:
+        import oracle as O
+
+        threads = O.hardware_threads()
+        ref, idx, cpu_s = cpu_oracle_sample(args.cpu_sample, threads)
+        headline["cpu_baseline"] = rounded({"value": args.cpu_sample / cpu_s / 1e6, "unit": "Mrays/s",
+                                            "cores": threads, "kind": "port",
+                                            "sample": f"{args.cpu_sample} seeded pixels, rtol 1e-10"})
 
     # ---- precision study on the same frame: plain FP32 and FP64 at the same job, errors vs the oracle
     if args.compare:
         comp = {}
-        ref = idx = None
-        if args.cpu_sample > 0:
-            import oracle as O
-
-            threads = O.hardware_threads()
-            ref, idx, cpu_s = cpu_oracle_sample(G, args.cpu_sample, threads)
-            line["cpu_baseline"] = {"value": args.cpu_sample / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
-                                    "kind": "port",
-                                    "sample": f"{args.cpu_sample} seeded pixels of the {WIDTH}x{HEIGHT} frame, "
-                                              "binary64 oracle rtol 1e-10 atol 1e-12"}
-            comp[args.precision] = error_report(G, d, ref, idx)
-            comp["reference_gpu_algorithm"] = reference_gpu_algorithm_report(G, ref, idx, threads)
+        if ref is not None:
+            comp[args.precision] = error_report(d, ref, idx)
+            comp["reference_gpu_algorithm"] = reference_gpu_algorithm_report(ref, idx, threads)
         shape = {k: policy[k] for k in ("persistent", "block_threads", "tile_w", "tile_h", "refill_interval",
                                          "rays_per_grab")}
         frame_tol = {k: policy[k] for k in ("position_rtol", "position_atol", "momentum_rtol", "momentum_atol",
@@ -419,7 +455,7 @@ def run_gpu(args) -> None:
                      "attempts_per_ray": float((dd["accepted_steps"] + dd["rejected_steps"]).mean()),
                      "policy": {k: getattr(pipe.policy, k) for k in ("position_rtol", "maximum_step")}}
             if ref is not None:
-                entry["error_vs_oracle"] = error_report(G, dd, ref, idx)
+                entry["error_vs_oracle"] = error_report(dd, ref, idx)
             comp[name] = entry
         # tolerance sweep: throughput against error for each mode, so that modes can be compared at
         # equal error (binary32 stepping stops improving at its rounding floor)
@@ -440,25 +476,30 @@ def run_gpu(args) -> None:
                     ms = a.elapsed_time(b)
                     dd = results.numpy()
                     sweep.append({"precision": name, "rtol": rtol, "mrays_per_s": rays / (ms / 1e3) / 1e6,
-                                  "error_vs_oracle": error_report(G, dd, ref, idx)})
+                                  "error_vs_oracle": error_report(dd, ref, idx)})
             comp["tolerance_sweep"] = sweep
         comp[args.precision] = {"mrays_per_s": value / world, "ms": total_ms / args.steps,
                                 "attempts_per_ray": float((d["accepted_steps"] + d["rejected_steps"]).mean()),
                                 "error_vs_oracle": comp.get(args.precision)}
-        line["precision_study"] = comp
+        studies["precision_study"] = comp
     if args.adjoint:
-        line["adjoint"] = adjoint_study(G, args, local)
+        studies["adjoint"] = adjoint_study(G, args, local)
     if args.batch:
-        line["batch"] = batch_study(G, local)
-        line["sky"] = sky_study(G, local)
+        studies["batch"] = batch_study(G, local)
+        studies["sky"] = sky_study(G, local)
     if args.footprint:
-        line["footprint"] = footprint_study(G, local, args.cpu_sample > 0)
+        studies["footprint"] = footprint_study(G, local, args.cpu_sample > 0)
     if args.scenes:
-        line["config1"] = config1_study(G, local, args.cpu_sample > 0)
-        line["scenes"] = scenes_study(G, local, args.cpu_sample > 0)
+        studies["config1"] = config1_study(G, local, args.cpu_sample > 0)
+        studies["scenes"] = scenes_study(G, local, args.cpu_sample > 0)
     if args.stress:
-        line["stress"] = stress_study(G, local, args.cpu_sample > 0, args.stress_side)
-    print(json.dumps(line), flush=True)
+        studies["stress"] = stress_study(G, local, args.cpu_sample > 0, args.stress_side)
+    # the studies go on earlier lines (and to --studies-out); the last line is the short headline
+    for name, study in studies.items():
+        print(json.dumps({"study": name, "result": study}), flush=True)
+    if args.studies_out:
+        Path(args.studies_out).write_text(json.dumps({"headline": headline, "studies": studies}, indent=1))
+    print(json.dumps(headline), flush=True)
     if dist:
         dist.destroy_process_group()
 
@@ -788,7 +829,7 @@ def scenes_study(G, device: int, cpu: bool) -> dict:
                 ms = timed_trace(pipe, [sc], cam, res, stream, flush)
                 entry = {"mrays_per_s": w * h / (ms / 1e3) / 1e6}
                 if ref is not None:
-                    entry["error_vs_oracle"] = error_report(G, res.numpy(), ref, idx)
+                    entry["error_vs_oracle"] = error_report(res.numpy(), ref, idx)
                 row[name] = entry
             rows.append(row)
     pipe.close()
@@ -844,7 +885,7 @@ def config1_study(G, device: int, cpu: bool) -> dict:
         ms = timed_trace(pipe, [sc], cam, res, stream, flush, reps=3)
         entry = {"ms": ms, "mrays_per_s": w * h / (ms / 1e3) / 1e6}
         if ref is not None:
-            entry["error_vs_oracle"] = error_report(G, res.numpy(), ref, idx)
+            entry["error_vs_oracle"] = error_report(res.numpy(), ref, idx)
         out[name] = entry
     pipe.close()
     return out
@@ -1079,6 +1120,8 @@ def main() -> None:
                     help="pixels of the frame traced by the CPU oracle (baseline and error report)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch from an ncu capture, reported as roofline.traffic")
+    ap.add_argument("--studies-out", default=None,
+                    help="also write the headline and every study to this JSON file")
     ap.add_argument("--width", type=int, default=WIDTH, help="frame width (smaller frames for profiling)")
     ap.add_argument("--height", type=int, default=HEIGHT, help="frame height")
     args = ap.parse_args()
