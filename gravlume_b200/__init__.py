@@ -7,6 +7,7 @@ host binding over that C ABI.
 """
 
 from ._native import RESULT_FIELDS, GlcError, lib  # noqa: F401
+from .batches import TileRegion, TraceProgress, tile_grid  # noqa: F401
 from .build import LIB_PATH, build  # noqa: F401
 from .trace import (  # noqa: F401
     EquatorialSurface, FootprintStatus, Graph, KerrSchildChart, Observation, Precision, ReferencePolicy, Termination,

@@ -11,7 +11,7 @@ c_double, c_int32, c_uint32, c_uint64, c_void_p = (ctypes.c_double, ctypes.c_int
                                                    ctypes.c_uint64, ctypes.c_void_p)
 
 GLC_OK = 0
-ABI_VERSION = 2  # GLC_ABI_VERSION of include/glc.h these structures mirror
+ABI_VERSION = 3  # GLC_ABI_VERSION of include/glc.h these structures mirror
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "NON_FINITE", 4: "NON_POSITIVE",
     5: "NON_NORMALIZED", 6: "EXTREMALITY_CHANGED", 7: "NON_STATIONARY", 8: "DEGENERATE_FRAME",
@@ -68,7 +68,7 @@ class Policy(ctypes.Structure):
         ("blocks_per_sm", c_uint32), ("tile_w", c_uint32), ("tile_h", c_uint32),
         ("refill_interval", c_uint32), ("rays_per_grab", c_uint32),
         ("refill_min_idle", c_uint32), ("mixed_pair_state", c_uint32), ("capture_certificates", c_uint32),
-        ("escape_map", c_uint32),
+        ("escape_map", c_uint32), ("mixed_split", c_uint32),
     ]
 
     def as_dict(self):
@@ -80,6 +80,7 @@ class Camera(ctypes.Structure):
         ("kind", c_int32), ("scene_index", c_int32), ("width", c_uint32), ("height", c_uint32),
         ("subpixel_x", c_double), ("subpixel_y", c_double), ("ray_states", c_void_p),
         ("n_rays", c_uint64), ("affine_direction", c_double), ("result_offset", c_uint64),
+        ("tile_origin", c_uint32 * 2), ("tile_count", c_uint32 * 2),
     ]
 
 

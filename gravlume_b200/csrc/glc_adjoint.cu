@@ -346,6 +346,8 @@ glc_status fill_tape(glc_tape* t, glc_ctx* ctx, const glc_adjoint_scene* as, con
   if (camera->kind != GLC_CAMERA_PINHOLE && camera->kind != GLC_CAMERA_RAYLIST)
     return set_error(GLC_ERR_UNSUPPORTED, "the adjoint takes a pinhole or ray-list camera");
   if (camera->scene_index != 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera must use scene 0");
+  if (camera->tile_count[0] != 0u || camera->tile_count[1] != 0u)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "the adjoint takes a whole-view camera (tile_count {0, 0})");
   if (!(as->observer_radius > 0.0) || !std::isfinite(as->observer_polar) || !std::isfinite(as->observer_azimuth))
     return set_error(GLC_ERR_INVALID_ARGUMENT, "observer oblate coordinates must be finite, radius positive");
   const double p0[4] = {as->input.spin, as->input.charge, as->observer_polar, as->observer_radius};

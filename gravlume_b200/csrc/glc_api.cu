@@ -64,6 +64,62 @@ struct JobLayout {
   size_t off_scenes = 0, off_cams = 0, off_begin = 0, off_cert_begin = 0, off_emap_begin = 0, bytes = 0;
 };
 
+// A camera's tile region (TileRegion, trace.rs:799-857): whole view ({0, 0} tiles), or a non-empty
+// block of 8x8-pixel tiles inside the view's tile grid (tile_grid, trace.rs:851-856).
+glc_status validate_region(const glc_camera& c) {
+  if (c.tile_count[0] == 0u && c.tile_count[1] == 0u) {
+    if (c.tile_origin[0] != 0u || c.tile_origin[1] != 0u)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "a whole-view camera has tile origin (0, 0)");
+    return GLC_OK;
+  }
+  if (c.kind == GLC_CAMERA_RAYLIST) return set_error(GLC_ERR_INVALID_ARGUMENT, "ray lists have no tile region");
+  const uint64_t gx = (uint64_t(c.width) + kRegionTile - 1) / kRegionTile;
+  const uint64_t gy = (uint64_t(c.height) + kRegionTile - 1) / kRegionTile;
+  if (c.tile_count[0] == 0u || c.tile_count[1] == 0u ||
+      uint64_t(c.tile_origin[0]) + c.tile_count[0] > gx || uint64_t(c.tile_origin[1]) + c.tile_count[1] > gy)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "tile region outside the view's tile grid");
+  return GLC_OK;
+}
+
+bool whole_view(const glc_camera& c) { return c.tile_count[0] == 0u && c.tile_count[1] == 0u; }
+
+}  // namespace
+
+// Rays of one camera under the policy's tile padding (its tile region for image cameras), with
+// the camera checks of every trace entry point.
+glc_status glc::camera_ray_count(const glc_camera& c, const glc_scene* scenes, int32_t n_scenes,
+                                 const glc_policy& pol, unsigned long long* n) {
+  if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
+  if (c.scene_index < 0 || c.scene_index >= n_scenes)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "camera scene index out of range");
+  const glc_status rs = validate_region(c);
+  if (rs != GLC_OK) return rs;
+  if (c.kind == GLC_CAMERA_RAYLIST) {
+    if (!c.ray_states && c.n_rays > 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "ray list needs states");
+    if (!(c.affine_direction == 1.0 || c.affine_direction == -1.0))
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "affine direction must be +1 or -1");
+    if ((reinterpret_cast<uintptr_t>(c.ray_states) & 15u) != 0)
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "ray states must be 16-byte aligned");
+    *n = c.n_rays;
+    return GLC_OK;
+  }
+  if (c.kind != GLC_CAMERA_PINHOLE && c.kind != GLC_CAMERA_EQUIRECT)
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown camera kind");
+  if (c.width == 0 || c.height == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera size must be nonzero");
+  if (!(c.subpixel_x >= 0.0 && c.subpixel_x <= 1.0 && c.subpixel_y >= 0.0 && c.subpixel_y <= 1.0))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "subpixel offsets must lie in [0, 1]");
+  if (c.kind == GLC_CAMERA_PINHOLE &&
+      (c.width != scenes[c.scene_index].width || c.height != scenes[c.scene_index].height))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "pinhole camera size must match the scene's view");
+  const PixelRect rc = camera_rect(c);
+  const unsigned long long tx = (rc.x1 - rc.x0 + pol.tile_w - 1) / pol.tile_w;
+  const unsigned long long ty = (rc.y1 - rc.y0 + pol.tile_h - 1) / pol.tile_h;
+  *n = tx * ty * pol.tile_w * pol.tile_h;
+  return GLC_OK;
+}
+
+namespace {
+
 glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cams, int32_t n_cams,
                         const glc_policy& pol, JobLayout& L) {
   if (!scenes || !cams || n_scenes <= 0 || n_cams <= 0)
@@ -75,29 +131,9 @@ glc_status validate_job(const glc_scene* scenes, int32_t n_scenes, const glc_cam
   unsigned long long acc = 0, tiles = 0, nodes = 0;
   for (int i = 0; i < n_cams; ++i) {
     const glc_camera& c = cams[i];
-    if (c.scene_index < 0 || c.scene_index >= n_scenes)
-      return set_error(GLC_ERR_INVALID_ARGUMENT, "camera scene index out of range");
     unsigned long long n = 0;
-    if (c.kind == GLC_CAMERA_RAYLIST) {
-      if (!c.ray_states && c.n_rays > 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "ray list needs states");
-      if (!(c.affine_direction == 1.0 || c.affine_direction == -1.0))
-        return set_error(GLC_ERR_INVALID_ARGUMENT, "affine direction must be +1 or -1");
-      if ((reinterpret_cast<uintptr_t>(c.ray_states) & 15u) != 0)
-        return set_error(GLC_ERR_INVALID_ARGUMENT, "ray states must be 16-byte aligned");
-      n = c.n_rays;
-    } else if (c.kind == GLC_CAMERA_PINHOLE || c.kind == GLC_CAMERA_EQUIRECT) {
-      if (c.width == 0 || c.height == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera size must be nonzero");
-      if (!(c.subpixel_x >= 0.0 && c.subpixel_x <= 1.0 && c.subpixel_y >= 0.0 && c.subpixel_y <= 1.0))
-        return set_error(GLC_ERR_INVALID_ARGUMENT, "subpixel offsets must lie in [0, 1]");
-      if (c.kind == GLC_CAMERA_PINHOLE &&
-          (c.width != scenes[c.scene_index].width || c.height != scenes[c.scene_index].height))
-        return set_error(GLC_ERR_INVALID_ARGUMENT, "pinhole camera size must match the scene's view");
-      const unsigned long long tx = (c.width + pol.tile_w - 1) / pol.tile_w;
-      const unsigned long long ty = (c.height + pol.tile_h - 1) / pol.tile_h;
-      n = tx * ty * pol.tile_w * pol.tile_h;
-    } else {
-      return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown camera kind");
-    }
+    const glc_status cs = camera_ray_count(c, scenes, n_scenes, pol, &n);
+    if (cs != GLC_OK) return cs;
     L.begin[i] = acc;
     acc += n;
     L.cert_begin[i] = tiles;
@@ -154,6 +190,7 @@ struct glc_graph {
   unsigned long long* d_queue = nullptr;
   uint32_t* d_cert = nullptr;
   uint32_t* d_emap = nullptr;
+  unsigned char* d_handoff = nullptr;
 };
 
 namespace {
@@ -196,11 +233,48 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
   return GLC_OK;
 }
 
+// MIXED as two kernels (binary32 bulk, then binary64 completion) over the hand-off records.
+bool split_mixed(const glc_policy& pol) {
+  return pol.precision == GLC_MIXED && pol.persistent == 0 && pol.mixed_split != 0;
+}
+
+size_t handoff_bytes(unsigned long long rays) { return size_t(rays) * kHandoffWords * sizeof(uint4); }
+
+glc_status launch_split(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out,
+                        cudaStream_t stream, unsigned char* handoff) {
+  const unsigned block = pol.block_threads;
+  const unsigned long long grid = (job.total + block - 1) / block;
+  if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
+  const Handoff hv{reinterpret_cast<uint4*>(handoff), job.total};
+  trace_bulk_kernel<kBULK><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
+  GLC_CUDA(cudaGetLastError());
+  trace_tail_kernel<kTAIL><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
+  GLC_CUDA(cudaGetLastError());
+  ctx->stats.last_grid = unsigned(grid);
+  ctx->stats.kernel_launches += 2;
+  ctx->stats.last_block = block;
+  ctx->stats.last_persistent = 0;
+  ctx->stats.last_rays = job.total;
+  return GLC_OK;
+}
+
+glc_status ensure_bytes(unsigned char** buf, size_t* have, size_t need) {
+  if (need <= *have) return GLC_OK;
+  if (*buf) GLC_CUDA(cudaFree(*buf));
+  *buf = nullptr;
+  *have = 0;
+  GLC_CUDA(cudaMalloc(buf, need));
+  *have = need;
+  return GLC_OK;
+}
+
 // cert: device words for the job's certificate tiles (at least cert_tiles of them) when the policy
-// asks for certificates, else unused.
+// asks for certificates, else unused. handoff: hand-off records for every ray of the job when the
+// policy splits MIXED into two kernels (without it the one-kernel MIXED runs).
 glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, const glc_results& out,
                   cudaStream_t stream, unsigned long long* queue, uint32_t* cert = nullptr,
-                  unsigned long long cert_tiles = 0, uint32_t* emap = nullptr, unsigned long long emap_nodes = 0) {
+                  unsigned long long cert_tiles = 0, uint32_t* emap = nullptr, unsigned long long emap_nodes = 0,
+                  unsigned char* handoff = nullptr) {
   if (job_in.total == 0) return GLC_OK;
   if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
     return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
@@ -222,6 +296,7 @@ glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, co
     ctx->stats.kernel_launches += 1;
     job.emap = emap;
   }
+  if (split_mixed(pol) && handoff) return launch_split(ctx, job, pol, out, stream, handoff);
   switch (pol.precision) {
     case GLC_FP32: return launch_precision<kFP32>(ctx, job, pol, out, stream, queue);
     case GLC_MIXED: return launch_precision<kMIXED>(ctx, job, pol, out, stream, queue);
@@ -292,6 +367,8 @@ constexpr unsigned long long kBandRays = 1ull << 19;  // split cameras of more t
 bool plan_bands(const glc_camera* cams, int32_t n_cams, const JobLayout& L, const glc_policy& pol,
                 std::vector<Band>& bands) {
   bands.clear();
+  for (int c = 0; c < n_cams; ++c)
+    if (!whole_view(cams[c])) return false;  // a tile region's slots are not contiguous rows
   for (int c = 0; c < n_cams; ++c) {
     const unsigned long long g = L.begin[c], rays = L.begin[c + 1] - g;
     if (rays == 0) continue;
@@ -324,6 +401,18 @@ void launch_band(const JobView& job, const glc_policy& pol, const glc_results& o
   trace_simple_kernel<P><<<unsigned(grid), pol.block_threads, 0, st>>>(jb, pol, out, b.g0);
 }
 
+// The two MIXED kernels on one band; the hand-off records are indexed by the job's ray index, so
+// bands in flight on different streams use disjoint records.
+void launch_band_split(const JobView& job, const glc_policy& pol, const glc_results& out, const Band& b,
+                       cudaStream_t st, unsigned char* handoff) {
+  JobView jb = job;
+  jb.total = b.g1;
+  const unsigned long long grid = (b.g1 - b.g0 + pol.block_threads - 1) / pol.block_threads;
+  const Handoff hv{reinterpret_cast<uint4*>(handoff), job.total};
+  trace_bulk_kernel<kBULK><<<unsigned(grid), pol.block_threads, 0, st>>>(jb, pol, out, hv, b.g0);
+  trace_tail_kernel<kTAIL><<<unsigned(grid), pol.block_threads, 0, st>>>(jb, pol, out, hv, b.g0);
+}
+
 glc_status ensure_host_streams(glc_ctx* ctx) {
   for (cudaStream_t& c : ctx->host_compute)
     if (!c) GLC_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
@@ -336,6 +425,8 @@ glc_status ensure_host_streams(glc_ctx* ctx) {
 }
 
 }  // namespace
+
+glc_status glc::check_policy(const glc_policy& p) { return validate_policy(p); }
 
 extern "C" {
 
@@ -447,6 +538,7 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
   p.mixed_pair_state = precision == GLC_MIXED ? 1u : 0u;
   p.capture_certificates = 0;
   p.escape_map = 0;
+  p.mixed_split = 1;
   *out = p;
   return GLC_OK;
 }
@@ -515,6 +607,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_shadow) cudaFree(ctx->d_shadow);
   if (ctx->d_footprint) cudaFree(ctx->d_footprint);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
+  if (ctx->d_handoff) cudaFree(ctx->d_handoff);
   for (cudaEvent_t e : ctx->host_band)
     if (e) cudaEventDestroy(e);
   if (ctx->host_entry) cudaEventDestroy(ctx->host_entry);
@@ -586,8 +679,12 @@ glc_status glc_trace(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes, co
     s = ensure_cert_capacity(&ctx->d_emap, &ctx->d_emap_words, nodes);
     if (s != GLC_OK) return s;
   }
+  if (split_mixed(ctx->policy)) {
+    s = ensure_bytes(&ctx->d_handoff, &ctx->d_handoff_bytes, handoff_bytes(L.total));
+    if (s != GLC_OK) return s;
+  }
   return launch(ctx, job_view(ctx->d_job, L, n_cameras), ctx->policy, *out, st, ctx->d_queue, ctx->d_cert, tiles,
-                ctx->d_emap, nodes);
+                ctx->d_emap, nodes, ctx->d_handoff);
 }
 
 glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scenes,
@@ -598,6 +695,9 @@ glc_status glc_refine_shadow_edges(glc_ctx* ctx, const glc_scene* scenes, int32_
   JobLayout L;
   glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
   if (s != GLC_OK) return s;
+  for (int i = 0; i < n_cameras; ++i)
+    if (!whole_view(cameras[i]))
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "shadow-edge refinement takes whole-view cameras (tile_count {0, 0})");
   s = ensure_job_capacity(ctx, L.bytes);
   if (s != GLC_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -658,6 +758,9 @@ glc_status glc_surface_footprint(glc_ctx* ctx, const glc_scene* scenes, int32_t 
   JobLayout L;
   glc_status s = validate_job(scenes, n_scenes, cameras, n_cameras, ctx->policy, L);
   if (s != GLC_OK) return s;
+  for (int i = 0; i < n_cameras; ++i)
+    if (!whole_view(cameras[i]))
+      return set_error(GLC_ERR_INVALID_ARGUMENT, "surface footprints take whole-view cameras (tile_count {0, 0})");
   s = ensure_job_capacity(ctx, L.bytes);
   if (s != GLC_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -775,6 +878,11 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     }
     s = ensure_job_capacity(ctx, L.bytes);
     if (s != GLC_OK) return s;
+    const bool split = split_mixed(pol);
+    if (split) {
+      s = ensure_bytes(&ctx->d_handoff, &ctx->d_handoff_bytes, handoff_bytes(L.total));
+      if (s != GLC_OK) return s;
+    }
     fill_staging(ctx->h_stage, L, scenes, n_scenes, cams.data(), n_cameras);
     GLC_CUDA(cudaMemcpyAsync(ctx->d_job, ctx->h_stage, L.bytes, cudaMemcpyHostToDevice, cs));
     GLC_CUDA(cudaEventRecord(ctx->stage_free, cs));
@@ -785,10 +893,15 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
     const JobView job = job_view(ctx->d_job, L, n_cameras);
     for (size_t k = 0; k < bands.size(); ++k) {
       cudaStream_t bs = (k & 1u) ? cs2 : cs;
-      switch (pol.precision) {
-        case GLC_FP32: launch_band<kFP32>(job, pol, dev, bands[k], bs); break;
-        case GLC_MIXED: launch_band<kMIXED>(job, pol, dev, bands[k], bs); break;
-        default: launch_band<kFP64>(job, pol, dev, bands[k], bs); break;
+      if (split) {
+        launch_band_split(job, pol, dev, bands[k], bs, ctx->d_handoff);
+        ctx->stats.kernel_launches += 1;
+      } else {
+        switch (pol.precision) {
+          case GLC_FP32: launch_band<kFP32>(job, pol, dev, bands[k], bs); break;
+          case GLC_MIXED: launch_band<kMIXED>(job, pol, dev, bands[k], bs); break;
+          default: launch_band<kFP64>(job, pol, dev, bands[k], bs); break;
+        }
       }
       GLC_CUDA(cudaGetLastError());
       GLC_CUDA(cudaEventRecord(ctx->host_band[k], bs));
@@ -823,9 +936,31 @@ glc_status glc_trace_host(glc_ctx* ctx, const glc_scene* scenes, int32_t n_scene
   }
   s = glc_trace(ctx, scenes, n_scenes, cams.data(), n_cameras, &dev, nullptr);
   if (s != GLC_OK) return s;
+  bool regions = false;
+  for (int i = 0; i < n_cameras; ++i) regions = regions || !whole_view(cams[i]);
   for (int i = 0; i < kFields; ++i) {
     if (!hfields[i]) continue;
-    GLC_CUDA(cudaMemcpyAsync(hfields[i], *dfields[i], slots * esize[i], cudaMemcpyDeviceToHost, nullptr));
+    if (!regions) {
+      GLC_CUDA(cudaMemcpyAsync(hfields[i], *dfields[i], slots * esize[i], cudaMemcpyDeviceToHost, nullptr));
+      continue;
+    }
+    // tile regions: copy back each camera's traced pixels only (the rest of the host arrays, which
+    // other batches fill, is left as it is)
+    for (int c = 0; c < n_cameras; ++c) {
+      const glc_camera& cm = cams[c];
+      unsigned char* h = static_cast<unsigned char*>(hfields[i]);
+      const unsigned char* d = static_cast<const unsigned char*>(*dfields[i]);
+      if (cm.kind == GLC_CAMERA_RAYLIST) {
+        const size_t off = cm.result_offset * esize[i];
+        if (cm.n_rays) GLC_CUDA(cudaMemcpyAsync(h + off, d + off, cm.n_rays * esize[i], cudaMemcpyDeviceToHost, nullptr));
+        continue;
+      }
+      const PixelRect rc = camera_rect(cm);
+      const size_t pitch = size_t(cm.width) * esize[i];
+      const size_t off = (cm.result_offset + size_t(rc.y0) * cm.width + rc.x0) * esize[i];
+      GLC_CUDA(cudaMemcpy2DAsync(h + off, pitch, d + off, pitch, size_t(rc.x1 - rc.x0) * esize[i], rc.y1 - rc.y0,
+                                 cudaMemcpyDeviceToHost, nullptr));
+    }
   }
   GLC_CUDA(cudaStreamSynchronize(nullptr));
   return GLC_OK;
@@ -850,6 +985,7 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
     if (G->d_queue) cudaFree(G->d_queue);
     if (G->d_cert) cudaFree(G->d_cert);
     if (G->d_emap) cudaFree(G->d_emap);
+    if (G->d_handoff) cudaFree(G->d_handoff);
     delete G;
     return st;
   };
@@ -858,7 +994,8 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
   if (cudaMalloc(&G->d_job, L.bytes) != cudaSuccess || cudaMallocHost(&G->h_stage, L.bytes) != cudaSuccess ||
       cudaMalloc(&G->d_queue, 256) != cudaSuccess ||
       (tiles && cudaMalloc(&G->d_cert, tiles * sizeof(uint32_t)) != cudaSuccess) ||
-      (nodes && cudaMalloc(&G->d_emap, nodes * sizeof(uint32_t)) != cudaSuccess))
+      (nodes && cudaMalloc(&G->d_emap, nodes * sizeof(uint32_t)) != cudaSuccess) ||
+      (split_mixed(ctx->policy) && cudaMalloc(&G->d_handoff, handoff_bytes(L.total)) != cudaSuccess))
     return fail(set_error(GLC_ERR_CUDA, "graph buffer allocation failed"));
   fill_staging(G->h_stage, L, scenes, n_scenes, cameras, n_cameras);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -866,7 +1003,7 @@ glc_status glc_graph_capture(glc_ctx* ctx, const glc_scene* scenes, int32_t n_sc
     return fail(set_error(GLC_ERR_CUDA, "cudaStreamBeginCapture failed"));
   cudaError_t ce = cudaMemcpyAsync(G->d_job, G->h_stage, L.bytes, cudaMemcpyHostToDevice, st);
   glc_status ls = ce == cudaSuccess ? launch(ctx, job_view(G->d_job, L, n_cameras), ctx->policy, *out, st, G->d_queue,
-                                           G->d_cert, tiles, G->d_emap, nodes)
+                                           G->d_cert, tiles, G->d_emap, nodes, G->d_handoff)
                                     : set_error(GLC_ERR_CUDA, cudaGetErrorString(ce));
   cudaGraph_t gr = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(st, &gr);
@@ -901,6 +1038,7 @@ glc_status glc_graph_destroy(glc_graph* graph) {
   if (graph->d_queue) cudaFree(graph->d_queue);
   if (graph->d_cert) cudaFree(graph->d_cert);
   if (graph->d_emap) cudaFree(graph->d_emap);
+  if (graph->d_handoff) cudaFree(graph->d_handoff);
   delete graph;
   return GLC_OK;
 }

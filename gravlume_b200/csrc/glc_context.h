@@ -28,6 +28,8 @@ struct glc_ctx {
   uint32_t* d_footprint = nullptr;     // surface-footprint pixel list: counter word pair, then u64 entries
   size_t d_footprint_words = 0;
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
+  unsigned char* d_handoff = nullptr;  // MIXED two-kernel hand-off records (grow-only)
+  size_t d_handoff_bytes = 0;
   cudaStream_t host_compute[2] = {};  // glc_trace_host: bands are traced on two streams in turn ...
   cudaStream_t host_copy = nullptr;    // ... and copied back on a third
   cudaEvent_t host_upload = nullptr;   // the job table is on the device

@@ -25,11 +25,21 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) escape_map_no
   const uint32_t W = cam.width, H = cam.height, gw = map_grid_w(W);
   const unsigned long long j = t - job.emap_begin[lo];
   const uint32_t px = uint32_t(j % gw) * kMapNodeStep, py = uint32_t(j / gw) * kMapNodeStep;
+  // a tile region needs the nodes of its 8x8 tiles' stencils, which reach one node row and column
+  // past its last tile; node pixels outside the region are traced for the map but not stored
+  const PixelRect rc = camera_rect(cam);
+  const bool whole = cam.tile_count[0] == 0u && cam.tile_count[1] == 0u;
+  const uint32_t xe = (whole ? (W + kRegionTile - 1) / kRegionTile : cam.tile_origin[0] + cam.tile_count[0]) * kRegionTile;
+  const uint32_t ye = (whole ? (H + kRegionTile - 1) / kRegionTile : cam.tile_origin[1] + cam.tile_count[1]) * kRegionTile;
+  if (px < rc.x0 || py < rc.y0 || px > xe || py > ye) return;
+  const bool store = px < rc.x1 && py < rc.y1;
+  glc_results none{};
+  const glc_results& dst = store ? out : none;
   uint32_t packed = 0u;
   if (px < W && py < H) {
     const unsigned long long slot = cam.result_offset + (unsigned long long)py * W + px;
     if (job.cert && job.cert[job.cert_begin[lo] + (unsigned long long)(py >> 4) * ((W + 15u) >> 4) + (px >> 4)]) {
-      write_certified(out, slot);
+      write_certified(dst, slot);
       packed = kMapTagHorizon << kMapTagShift;
     } else {
       const glc_scene& sc = job.scenes[cam.scene_index];
@@ -44,7 +54,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) escape_map_no
         if (P == kMIXED) use64 = __any_sync(__activemask(), double(ray.r) < ls.shell_r);
         if (ray_step<P>(ray, ls, pol, res, use64)) break;
       }
-      write_result<P>(out, slot, ray, res, ls);
+      write_result<P>(dst, slot, ray, res, ls);
       if (res.termination == GLC_TERM_ESCAPE) {
         const double th = double(res.escape_theta), ph = double(res.escape_phi);
         if (isfinite(th) && isfinite(ph)) {

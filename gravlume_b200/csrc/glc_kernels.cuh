@@ -9,6 +9,21 @@
 
 namespace glc {
 
+// Pixel rectangle [x0, x1) x [y0, y1) an image camera traces: its tile region of 8x8-pixel tiles
+// (TileRegion, crates/gravlume-render/src/trace.rs:799-857, TRACE_WORKGROUP_AXIS = 8), or the whole
+// view when tile_count is {0, 0}. The host validates the region against the view's tile grid.
+constexpr uint32_t kRegionTile = 8;
+struct PixelRect {
+  uint32_t x0, y0, x1, y1;
+};
+__host__ __device__ __forceinline__ PixelRect camera_rect(const glc_camera& c) {
+  if (c.tile_count[0] == 0u && c.tile_count[1] == 0u) return {0u, 0u, c.width, c.height};
+  const uint32_t x0 = c.tile_origin[0] * kRegionTile, y0 = c.tile_origin[1] * kRegionTile;
+  const uint32_t x1 = (c.tile_origin[0] + c.tile_count[0]) * kRegionTile;
+  const uint32_t y1 = (c.tile_origin[1] + c.tile_count[1]) * kRegionTile;
+  return {x0, y0, x1 < c.width ? x1 : c.width, y1 < c.height ? y1 : c.height};
+}
+
 // Device view of one trace job: scenes, cameras and the prefix of their (padded) ray counts.
 struct JobView {
   const glc_scene* scenes;
@@ -154,14 +169,15 @@ __device__ __forceinline__ bool ray_setup(const JobView& job, const glc_policy& 
     return true;
   }
   const uint32_t W = cam->width, H = cam->height;
+  const PixelRect rc = camera_rect(*cam);
   const uint32_t tw = pol.tile_w, th = pol.tile_h;
-  const uint32_t tiles_x = (W + tw - 1) / tw;
+  const uint32_t tiles_x = (rc.x1 - rc.x0 + tw - 1) / tw;
   const unsigned long long per_tile = (unsigned long long)tw * th;
   const unsigned long long tile = j / per_tile;
   const uint32_t within = uint32_t(j - tile * per_tile);
-  const uint32_t px = uint32_t(tile % tiles_x) * tw + within % tw;
-  const uint32_t py = uint32_t(tile / tiles_x) * th + within / tw;
-  if (px >= W || py >= H) return false;
+  const uint32_t px = rc.x0 + uint32_t(tile % tiles_x) * tw + within % tw;
+  const uint32_t py = rc.y0 + uint32_t(tile / tiles_x) * th + within / tw;
+  if (px >= rc.x1 || py >= rc.y1) return false;
   slot = cam->result_offset + (unsigned long long)py * W + px;
   dir = -1.0;
   if (job.cert) {
@@ -345,10 +361,14 @@ __device__ __forceinline__ void write_reconstructed(const glc_results& o, unsign
 #ifndef GLC_MIN_BLOCKS_FP64
 #define GLC_MIN_BLOCKS_FP64 2
 #endif
+#ifndef GLC_MIN_BLOCKS_BULK
+#define GLC_MIN_BLOCKS_BULK 4
+#endif
 template <int P>
 struct LaunchShape {
   static constexpr int kMinBlocks =
-      P == kFP32 ? GLC_MIN_BLOCKS_FP32 : (P == kMIXED ? GLC_MIN_BLOCKS_MIXED : GLC_MIN_BLOCKS_FP64);
+      (P == kFP32 || P == kBULK) ? (P == kFP32 ? GLC_MIN_BLOCKS_FP32 : GLC_MIN_BLOCKS_BULK)
+                                 : (P == kMIXED ? GLC_MIN_BLOCKS_MIXED : GLC_MIN_BLOCKS_FP64);
 };
 
 template <int P>
@@ -391,6 +411,93 @@ template <int P>
 __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_simple_kernel(JobView job, glc_policy pol, glc_results out,
                                                                                        unsigned long long base) {
   trace_one<P>(job, pol, out, base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---- MIXED as two kernels: the hand-off records (HandoffRec, glc_tracer.cuh) of a job's rays are
+// stored word-major, word w of ray gi at rec[w * n + gi], so that a warp's stores and loads of one
+// word are contiguous 16-byte accesses.
+struct Handoff {
+  uint4* rec;
+  unsigned long long n;  // rays of the job (the stride between words)
+};
+constexpr int kHandoffWords = int(sizeof(HandoffRec) / sizeof(uint4));
+
+__device__ __forceinline__ void handoff_store(const Handoff& hv, unsigned long long gi, const Ray<kBULK>& ray,
+                                              const RayResult<float>& res) {
+  HandoffRec rec;
+  handoff_pack(ray, res, rec);
+  const uint4* w = reinterpret_cast<const uint4*>(&rec);
+#pragma unroll
+  for (int k = 0; k < kHandoffWords; ++k) hv.rec[k * hv.n + gi] = w[k];
+}
+
+__device__ __forceinline__ uint32_t handoff_resume(const Handoff& hv, unsigned long long gi, Ray<kTAIL>& ray,
+                                                   const LaneScene& sc, const double st8[8], double direction,
+                                                   uint32_t& failure) {
+  HandoffRec rec;
+  uint4* w = reinterpret_cast<uint4*>(&rec);
+#pragma unroll
+  for (int k = 0; k < kHandoffWords; ++k) w[k] = hv.rec[k * hv.n + gi];
+  return handoff_unpack(rec, ray, sc, st8, direction, failure);
+}
+
+// MIXED, first kernel: one thread per ray, binary32 stepping with the compensated pair state at
+// the binary32 register budget. Non-terminal turning points and equatorial crossings are handled
+// here; a ray leaves at the start of its first step that brackets a terminal event (or a surface
+// crossing near the surface), or when it enters the binary64 shell, or when it fails, by storing
+// its hand-off record. Certified and map-reconstructed pixels are written here.
+template <int P = kBULK>
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
+    trace_bulk_kernel(JobView job, glc_policy pol, glc_results out, Handoff hv, unsigned long long base) {
+  static_assert(P == kBULK, "the bulk kernel steps the BULK precision");
+  const unsigned long long gi = base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= job.total) return;
+  double st8[8], dir;
+  unsigned long long slot;
+  int scene_idx, shortcut;
+  double rdir[3];
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) return;
+  if (shortcut != kShortNone) {
+    if (shortcut == kShortCertified) write_certified(out, slot);
+    else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
+    return;
+  }
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+  Ray<kBULK> ray;
+  ray.init(ls, pol, st8, dir);
+  RayResult<float> res;
+  while (!ray.step(ls, pol, res, false)) {
+  }
+  handoff_store(hv, gi, ray, res);
+}
+
+// MIXED, second kernel: one thread per ray of the same job; resumes each handed-off ray in binary64
+// (re-taking the step it left at, with binary64 error control, root-finding and observables, the
+// shell steps, and the renormalization of the final momentum) and writes its result.
+template <int P = kTAIL>
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
+    trace_tail_kernel(JobView job, glc_policy pol, glc_results out, Handoff hv, unsigned long long base) {
+  static_assert(P == kTAIL, "the completion kernel steps the TAIL precision");
+  const unsigned long long gi = base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= job.total) return;
+  double st8[8], dir;
+  unsigned long long slot;
+  int scene_idx, shortcut;
+  double rdir[3];
+  if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) return;
+  if (shortcut != kShortNone) return;
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+  Ray<kTAIL> ray;
+  uint32_t failure = GLC_FAIL_NONE;
+  const uint32_t term = handoff_resume(hv, gi, ray, ls, st8, dir, failure);
+  RayResult<double> res;
+  if (term != GLC_TERM_NONE) {
+    ray.finish_plain(res, term, failure);
+  } else {
+    while (!ray.step(ls, pol, res, false)) {
+    }
+  }
+  write_result<kTAIL>(out, slot, ray, res, ls);
 }
 
 // Work-queue kernel with warp-granular grabs: a grid of SMs x occupancy whose warps take

@@ -42,11 +42,21 @@ unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 constexpr size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device, looked up on the first call on the
+// device. A cached address is checked before use: after a cudaDeviceReset the library's module is
+// loaded again and the array may live elsewhere, and then the address is looked up anew.
 glc_status scratch_address(int device, unsigned char** out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[device]) {
-    unsigned char* ptr = nullptr;
+  unsigned char* ptr = g_scratch_ptr[device];
+  if (ptr) {
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, ptr);
+    if (e != cudaSuccess || attr.type != cudaMemoryTypeDevice || attr.device != device) {
+      cudaGetLastError();
+      ptr = nullptr;
+    }
+  }
+  if (!ptr) {
     const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_trace_scratch);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -54,35 +64,7 @@ glc_status scratch_address(int device, unsigned char** out) {
     }
     g_scratch_ptr[device] = ptr;
   }
-  *out = g_scratch_ptr[device];
-  return GLC_OK;
-}
-
-// Ray count of one camera under the policy's tile padding, with the checks glc_trace applies.
-glc_status camera_rays(const glc_camera& c, const glc_scene* scenes, int32_t n_scenes, const glc_policy& pol,
-                       unsigned long long* n) {
-  if (c.scene_index < 0 || c.scene_index >= n_scenes)
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "camera scene index out of range");
-  if (c.kind == GLC_CAMERA_RAYLIST) {
-    if (!c.ray_states && c.n_rays > 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "ray list needs states");
-    if (!(c.affine_direction == 1.0 || c.affine_direction == -1.0))
-      return set_error(GLC_ERR_INVALID_ARGUMENT, "affine direction must be +1 or -1");
-    if ((reinterpret_cast<uintptr_t>(c.ray_states) & 15u) != 0)
-      return set_error(GLC_ERR_INVALID_ARGUMENT, "ray states must be 16-byte aligned");
-    *n = c.n_rays;
-    return GLC_OK;
-  }
-  if (c.kind != GLC_CAMERA_PINHOLE && c.kind != GLC_CAMERA_EQUIRECT)
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown camera kind");
-  if (c.width == 0 || c.height == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "camera size must be nonzero");
-  if (!(c.subpixel_x >= 0.0 && c.subpixel_x <= 1.0 && c.subpixel_y >= 0.0 && c.subpixel_y <= 1.0))
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "subpixel offsets must lie in [0, 1]");
-  if (c.kind == GLC_CAMERA_PINHOLE &&
-      (c.width != scenes[c.scene_index].width || c.height != scenes[c.scene_index].height))
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "pinhole camera size must match the scene's view");
-  const unsigned long long tx = (c.width + pol.tile_w - 1) / pol.tile_w;
-  const unsigned long long ty = (c.height + pol.tile_h - 1) / pol.tile_h;
-  *n = tx * ty * pol.tile_w * pol.tile_h;
+  *out = ptr;
   return GLC_OK;
 }
 
@@ -90,20 +72,32 @@ template <int P>
 glc_status launch_static(int device, const JobView& job, const glc_policy& pol, const glc_results& out,
                          cudaStream_t stream, unsigned long long* queue) {
   const unsigned block = pol.block_threads;
-  int per_sm = int(pol.blocks_per_sm);
-  if (per_sm <= 0) {
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<P>, int(block), 0);
-    if (e != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(e));
-    if (per_sm <= 0) per_sm = 1;
+  if (pol.persistent == 0) {
+    const unsigned long long grid = (job.total + block - 1) / block;
+    if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
+    trace_simple_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, 0ull);
+  } else {
+    int per_sm = int(pol.blocks_per_sm);
+    if (per_sm <= 0) {
+      const cudaError_t e =
+          pol.persistent == 2
+              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_queue_kernel<P>, int(block), 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<P>, int(block), 0);
+      if (e != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(e));
+      if (per_sm <= 0) per_sm = 1;
+    }
+    int sms = 0;
+    const cudaError_t ea = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (ea != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(ea));
+    const unsigned long long warps_needed = (job.total + 31) / 32;
+    unsigned long long grid = (unsigned long long)sms * per_sm;
+    const unsigned long long grid_cap = (warps_needed * 32 + block - 1) / block;
+    if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
+    if (pol.persistent == 2)
+      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+    else
+      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
   }
-  int sms = 0;
-  const cudaError_t ea = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (ea != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(ea));
-  const unsigned long long warps_needed = (job.total + 31) / 32;
-  unsigned long long grid = (unsigned long long)sms * per_sm;
-  const unsigned long long grid_cap = (warps_needed * 32 + block - 1) / block;
-  if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
-  trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(e));
   return GLC_OK;
@@ -120,19 +114,12 @@ extern "C" glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t 
     return set_error(GLC_ERR_CAPACITY,
                      "glc_trace_static_scratch takes at most 128 scenes and 128 cameras (96 KiB of static scratch)");
   const glc_policy& pol = *policy;
-  if (pol.tile_w == 0 || pol.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
-  if (pol.block_threads == 0 || pol.block_threads % 32 != 0 || pol.block_threads > 128)
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
-  if (pol.precision < GLC_FP32 || pol.precision > GLC_FP64)
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown precision mode");
-  const double positive[] = {pol.position_rtol, pol.position_atol, pol.momentum_rtol, pol.momentum_atol,
-                             pol.initial_step,  pol.minimum_step,  pol.maximum_step,  pol.safety,
-                             pol.minimum_factor, pol.maximum_factor, pol.event_affine_tolerance,
-                             pol.singularity_guard};
-  for (double x : positive)
-    if (!(x > 0.0) || !(x < 1.0e300)) return set_error(GLC_ERR_INVALID_ARGUMENT, "policy values must be positive");
-  if (pol.minimum_step > pol.maximum_step || pol.maximum_accepted_steps == 0 || pol.maximum_consecutive_rejects == 0)
-    return set_error(GLC_ERR_INVALID_ARGUMENT, "inconsistent step limits");
+  glc_status ps = check_policy(pol);
+  if (ps != GLC_OK) return ps;
+  if (pol.capture_certificates || pol.escape_map)
+    return set_error(GLC_ERR_INVALID_ARGUMENT,
+                     "glc_trace_static_scratch has no certificate or escape-map buffers: set capture_certificates "
+                     "and escape_map to 0");
 
   // Job table, laid out in a host buffer of the scratch's size (no allocation on either side).
   const size_t off_scenes = 0;
@@ -146,7 +133,7 @@ extern "C" glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t 
   unsigned long long acc = 0;
   for (int i = 0; i < n_cameras; ++i) {
     unsigned long long n = 0;
-    const glc_status s = camera_rays(cameras[i], scenes, n_scenes, pol, &n);
+    const glc_status s = camera_ray_count(cameras[i], scenes, n_scenes, pol, &n);
     if (s != GLC_OK) return s;
     begin[i] = acc;
     acc += n;

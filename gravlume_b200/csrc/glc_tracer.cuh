@@ -15,6 +15,11 @@
 //   FP32:  S = C = float.   FP64: S = C = double.
 //   MIXED: S = double, C = float; a warp whose lanes are inside the shell r < shell radius steps
 //          in double; the event path and the final null-constraint renormalisation are double.
+//   MIXED as two kernels (the frame path): BULK steps in binary32 with the compensated pair state
+//          (S = C = float) and leaves a ray at its first step that brackets a terminal event, or
+//          when it enters the shell; TAIL (S = C = double) resumes the ray from its hand-off
+//          record, re-takes that step, and finishes the trace in binary64 (event root-finding,
+//          shell steps, observables and the null-constraint renormalisation).
 #pragma once
 
 #include <type_traits>
@@ -33,7 +38,7 @@
 
 namespace glc {
 
-enum Prec : int { kFP32 = 0, kMIXED = 1, kFP64 = 2 };
+enum Prec : int { kFP32 = 0, kMIXED = 1, kFP64 = 2, kBULK = 3, kTAIL = 4 };
 
 template <int P>
 struct PrecTraits;
@@ -52,6 +57,23 @@ struct PrecTraits<kFP64> {
   using S = double;
   using C = double;
 };
+template <>
+struct PrecTraits<kBULK> {
+  using S = float;
+  using C = float;
+};
+template <>
+struct PrecTraits<kTAIL> {
+  using S = double;
+  using C = double;
+};
+
+// BULK hands a surface crossing to TAIL when its binary32 root radius lies within this relative
+// margin of the surface's radial interval, so that TAIL's binary64 root decides hits near the edges.
+constexpr double kBulkSurfaceMargin = 1e-4;
+// BULK localizes its non-terminal roots (radial turning points, equatorial crossings off the
+// surface) to at least this affine tolerance: binary32 cannot resolve the binary64 presets' 2e-11.
+constexpr double kBulkRootTolerance = 1e-6;
 
 enum EventBit : uint32_t { kEvGuard = 0, kEvHorizon = 1, kEvSurface = 2, kEvEscape = 3 };
 
@@ -388,7 +410,7 @@ template <int P>
 struct Ray {
   using S = typename PrecTraits<P>::S;
   using C = typename PrecTraits<P>::C;
-  static constexpr bool kPair = P == kMIXED;
+  static constexpr bool kPair = P == kMIXED || P == kBULK;
   using StepOut = StepOutT<C>;
 
   C yh[6], yl[6];  // state (yl: MIXED low parts, zero otherwise)
@@ -416,23 +438,26 @@ struct Ray {
   GLC_HD void state_s(S out[6]) const {
     for (int c = 0; c < 6; ++c) out[c] = ys(c);
   }
-  GLC_HD void set_state(const S v[6]) {
+  template <class V>
+  GLC_HD void set_state(const V v[6]) {
     for (int c = 0; c < 6; ++c) {
       yh[c] = C(v[c]);
-      yl[c] = kPair ? C(v[c] - S(yh[c])) : C(0);
+      yl[c] = kPair && pair ? C(v[c] - V(yh[c])) : C(0);
     }
   }
   GLC_HD S travel() const { return S(dir) * (S(th) + S(tl)); }
   GLC_HD S affine() const { return kPair ? S(ah) + S(al) : S(ah); }
 
   GLC_HD void init(const LaneScene& sc, const glc_policy& pol, const double st8[8], double direction) {
-    S v[6];
+    // the pair state splits the binary64 initial state into high and low parts
+    using V = typename std::conditional<kPair, double, S>::type;
+    V v[6];
     for (int c = 0; c < 3; ++c) {
-      v[c] = S(st8[1 + c]);
-      v[3 + c] = S(st8[5 + c]);
+      v[c] = V(st8[1 + c]);
+      v[3 + c] = V(st8[5 + c]);
     }
-    set_state(v);
     pair = kPair && pol.mixed_pair_state != 0u;
+    set_state(v);
     E = S(-st8[4]);
     Ec = C(E);
     dir = C(direction);
@@ -444,7 +469,7 @@ struct Ray {
     flags = 0;
     polar = st8[3] > 0.0 ? 1 : (st8[3] < 0.0 ? -1 : 0);
     turn_r = C(NAN);
-    az0 = g_atan2(v[1], v[0]);
+    az0 = P == kBULK ? S(0) : S(g_atan2(v[1], v[0]));  // BULK: the completion kernel derives it
     dnull = dlz = dq = C(0);
     // first derivative (FSAL seed), the invariants at the start and the event arming
     // (geodesic.rs:98-136, 536-544)
@@ -532,6 +557,7 @@ struct Ray {
       finish_plain(res, GLC_TERM_STEP_EXHAUSTION, GLC_FAIL_NONE);
       return true;
     }
+    if (P == kBULK && double(r) < sc.shell_r) return hand_off(res);
     const Tolerance tol{pol.position_rtol, pol.position_atol, pol.momentum_rtol, pol.momentum_atol};
     StepOut o;
     bool finite;
@@ -586,12 +612,6 @@ struct Ray {
       h = dir * next_step(pol, g_abs(h), o.en, false);
       return false;
     }
-    accepted += 1;
-    consecutive = 0;
-    if (stepped64) {
-      f64steps += 1;
-      flags |= kFlagShellF64;
-    }
     // ---- crossing detection in the stepping precision; the start values are exactly the
     // previous step's end values, so every sign change between consecutive states is seen
     const double guard = pol.singularity_guard;
@@ -613,6 +633,16 @@ struct Ray {
     if ((vs < C(0) && ve >= C(0)) || (vs > C(0) && ve <= C(0))) ev |= 1u << 4;
     if (event_crosses(kEvSurface, o.z0, o.z1)) ev |= 1u << 5;
     o.mask = ev;
+    // BULK: a step that brackets a root of the singularity guard, the horizon or the escape sphere
+    // is terminal whatever comes first in it; TAIL re-takes it in binary64
+    constexpr uint32_t kTerminalBits = (1u << kEvGuard) | (1u << kEvHorizon) | (1u << kEvEscape);
+    if (P == kBULK && (ev & kTerminalBits) != 0u) return hand_off(res);
+    accepted += 1;
+    consecutive = 0;
+    if (stepped64 || P == kTAIL) {
+      f64steps += 1;
+      flags |= kFlagShellF64;
+    }
     if (ev != 0u) {
       o.stepped64 = stepped64;
       // inline: with the streaming attempt the ray fits in registers, and copying it to local
@@ -710,11 +740,13 @@ struct Ray {
     }
     const T hh = T(h);
     const double guard = pol.singularity_guard;
-    const T tol = T(pol.event_affine_tolerance);
+    const T tol = T(P == kBULK && pol.event_affine_tolerance < kBulkRootTolerance ? kBulkRootTolerance
+                                                                                 : pol.event_affine_tolerance);
     int n = 0;
     int kinds[4];
     T thetas[4], residuals[4], states[4][6];
     for (int kind = 0; kind < 4; ++kind) {
+      if (P == kBULK && kind != kEvSurface) continue;  // the other events were handed off already
       if (!((o.mask >> kind) & 1u)) continue;
       const T sv = T(event_value<C>(kind, sc, guard, r, o.z0));
       const T evv = T(event_value<C>(kind, sc, guard, o.r_end, o.z1));
@@ -739,7 +771,11 @@ struct Ray {
       if (kind == kEvSurface) {
         int gs;
         const T rr = kn_radius(kt, yr[0], yr[1], yr[2], gs);
-        keep = gs == kGeomOk && rr >= T(sc.surf_in) && rr <= T(sc.surf_out);
+        if (P == kBULK)
+          keep = gs == kGeomOk && rr >= T(sc.surf_in * (1.0 - kBulkSurfaceMargin)) &&
+                 rr <= T(sc.surf_out * (1.0 + kBulkSurfaceMargin));
+        else
+          keep = gs == kGeomOk && rr >= T(sc.surf_in) && rr <= T(sc.surf_out);
       }
       if (keep) {
         kinds[n] = kind;
@@ -757,6 +793,11 @@ struct Ray {
       for (int i = 0; i < n; ++i)
         if (g_abs(thetas[i] - thetas[first]) * g_abs(hh) <= T(pol.event_tie_tolerance)) cand |= 1u << kinds[i];
     const bool has_event = first >= 0;
+    if (P == kBULK && has_event) {
+      // a surface crossing at or near the surface: TAIL re-takes the step (not counted here)
+      accepted -= 1;
+      return hand_off(res);
+    }
     const T term_theta = has_event ? thetas[first] : T(1);
     // radial turning point (geodesic.rs:330-360)
     if ((o.mask >> 4) & 1u) {
@@ -788,7 +829,7 @@ struct Ray {
       if (localize(y, hh, dpoly, tol, T(o.z0), T(o.z1), z_at, th_, yr, br) && (!has_event || th_ < term_theta))
         crossings += 1;
     }
-    if (!has_event) return false;
+    if (P == kBULK || !has_event) return false;
     // terminal commit at the event (precision S)
     T ycommit[6], dtc;
     {
@@ -815,6 +856,13 @@ struct Ray {
     return true;
   }
 
+  // BULK: leave the ray to TAIL at the current state (termination NONE: not finished).
+  GLC_HD bool hand_off(RayResult<S>& res) {
+    res.termination = GLC_TERM_NONE;
+    res.failure = GLC_FAIL_NONE;
+    return true;
+  }
+
   GLC_HD void finish_plain(RayResult<S>& res, uint32_t term, uint32_t failure) {
     res.termination = term;
     res.failure = failure;
@@ -833,7 +881,7 @@ struct Ray {
     const KN<T> kt = kn_cast<T>(sc.kn);
     T ye[6];
     for (int c = 0; c < 6; ++c) ye[c] = ystate[c];
-    if (P == kMIXED && pol.renormalize_null) {
+    if ((P == kMIXED || P == kTAIL) && pol.renormalize_null) {
       if (renormalize_null(kt, ye, E)) flags |= kFlagRenormalized;
     }
     res.termination = term;
@@ -870,5 +918,89 @@ struct Ray {
     res.flags = flags;
   }
 };
+
+// ---- MIXED as two kernels: the hand-off record of a ray from BULK to TAIL, 128 bytes (8 words of
+// 16 bytes, which the kernels store word-major across the job's rays):
+//   d[0..5] the state (x, y, z, p_x, p_y, p_z) in binary64 (the sum of the compensated pair),
+//   d[6] the affine parameter, d[7] the coordinate-time increment sum;
+//   f[0..7] step size with direction, L_z and Carter's constant at the start, minimum turning radius,
+//   the null residual, L_z and Carter drift maxima, unused;
+//   u[0..7] accepted, rejected, consecutive rejects, armed event bits, radial turnings, equatorial
+//   crossings, winding, and polar side + 1 | flags << 4 | termination << 16 | failure << 24 |
+//   invariants valid << 31.
+// E, the initial azimuth and the direction are not stored: TAIL re-derives them from the ray's
+// initial state, exactly as BULK did.
+struct alignas(16) HandoffRec {
+  double d[8];
+  float f[8];
+  uint32_t u[8];
+};
+static_assert(sizeof(HandoffRec) == 128, "hand-off record is 8 words of 16 bytes");
+
+GLC_HD void handoff_pack(const Ray<kBULK>& ray, const RayResult<float>& res, HandoffRec& rec) {
+  for (int c = 0; c < 6; ++c) rec.d[c] = double(ray.yh[c]) + double(ray.yl[c]);
+  rec.d[6] = double(ray.ah) + double(ray.al);
+  rec.d[7] = double(ray.th) + double(ray.tl);
+  rec.f[0] = ray.h;
+  rec.f[1] = ray.lz0;
+  rec.f[2] = ray.q0;
+  rec.f[3] = ray.turn_r;
+  rec.f[4] = ray.dnull;
+  rec.f[5] = ray.dlz;
+  rec.f[6] = ray.dq;
+  rec.f[7] = 0.0f;
+  rec.u[0] = ray.accepted;
+  rec.u[1] = ray.rejected;
+  rec.u[2] = ray.consecutive;
+  rec.u[3] = ray.armed;
+  rec.u[4] = ray.turnings;
+  rec.u[5] = ray.crossings;
+  rec.u[6] = uint32_t(ray.winding);
+  rec.u[7] = uint32_t(ray.polar + 1) | ((ray.flags & 0xFFFu) << 4) | ((res.termination & 0xFFu) << 16) |
+             ((res.failure & 0xFu) << 24) | (ray.have_inv ? 1u << 31 : 0u);
+}
+
+// Resume a handed-off ray as a binary64 stepper: the stored state and counters, E and the initial
+// azimuth from the ray's initial state st8, and the derivative, radius and radial velocity at the
+// state re-evaluated in binary64. Returns the termination BULK recorded (NONE: continue stepping)
+// and sets its failure kind.
+GLC_HD uint32_t handoff_unpack(const HandoffRec& rec, Ray<kTAIL>& ray, const LaneScene& sc, const double st8[8],
+                               double direction, uint32_t& failure) {
+  ray.pair = false;
+  ray.set_state(rec.d);
+  ray.E = -st8[4];
+  ray.Ec = ray.E;
+  ray.dir = direction;
+  ray.az0 = g_atan2(st8[2], st8[1]);
+  ray.ah = rec.d[6];
+  ray.al = 0.0;
+  ray.th = rec.d[7];
+  ray.tl = 0.0;
+  ray.h = double(rec.f[0]);
+  ray.lz0 = double(rec.f[1]);
+  ray.q0 = double(rec.f[2]);
+  ray.turn_r = double(rec.f[3]);
+  ray.dnull = double(rec.f[4]);
+  ray.dlz = double(rec.f[5]);
+  ray.dq = double(rec.f[6]);
+  ray.accepted = rec.u[0];
+  ray.rejected = rec.u[1];
+  ray.consecutive = rec.u[2];
+  ray.armed = rec.u[3];
+  ray.f64steps = 0;
+  ray.turnings = rec.u[4];
+  ray.crossings = rec.u[5];
+  ray.winding = int32_t(rec.u[6]);
+  const uint32_t w = rec.u[7];
+  ray.polar = int32_t(w & 0xFu) - 1;
+  ray.flags = (w >> 4) & 0xFFFu;
+  ray.have_inv = (w >> 31) != 0u;
+  failure = (w >> 24) & 0xFu;
+  double rr, vv;
+  kn_rhs(sc.kn, ray.yh, ray.Ec, ray.k1, rr, vv);
+  ray.r = rr;
+  ray.vr = vv;
+  return (w >> 16) & 0xFFu;
+}
 
 }  // namespace glc

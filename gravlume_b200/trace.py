@@ -342,12 +342,17 @@ class Graph:
 
 
 def image_camera(scene_index: int, width: int, height: int, subpixel=(0.5, 0.5), offset: int = 0,
-                 kind: int = N.CAMERA_PINHOLE) -> N.Camera:
+                 kind: int = N.CAMERA_PINHOLE, region=None) -> N.Camera:
+    """An image camera; `region` (a batches.TileRegion) limits the trace to a block of 8x8-pixel
+    tiles, written in the whole view's result layout."""
     c = N.Camera()
     c.kind, c.scene_index, c.width, c.height = kind, scene_index, width, height
     c.subpixel_x, c.subpixel_y = subpixel
     c.affine_direction = -1.0
     c.result_offset = offset
+    if region is not None:
+        c.tile_origin[:] = list(region.origin)
+        c.tile_count[:] = list(region.workgroups)
     return c
 
 
@@ -432,6 +437,35 @@ class TracePipeline:
         N.check(N.lib().glc_trace(self._h, sa, len(scenes), ca, len(cameras), ctypes.byref(rs),
                                   self._stream(stream)), "glc_trace")
         return results
+
+    def trace_progressive(self, scenes: Sequence[N.Scene], camera: N.Camera, results: TraceResults | None = None,
+                          stream=None, progress=None):
+        """Trace one whole-view image camera in tile batches, as the reference's renderer advances a
+        frame (Renderer::advance_trace, crates/gravlume-render/src/renderer.rs:470-506, with the
+        TraceProgress schedule of renderer/frame.rs:326-420): each batch is a glc_trace of the
+        camera's tile region, timed with CUDA events on the stream, and its time rescales the next
+        batch's tile budget. Returns the results and the list of (TileRegion, ms)."""
+        torch = _torch()
+        from .batches import TraceProgress
+        from .trace import image_camera as _cam
+        if results is None:
+            results = TraceResults(self.result_slots(scenes, [camera]), torch.device("cuda", self.device))
+        progress = progress or TraceProgress(camera.width, camera.height)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        done = []
+        while (batch := progress.next_batch()) is not None:
+            cam = _cam(camera.scene_index, camera.width, camera.height, (camera.subpixel_x, camera.subpixel_y),
+                       camera.result_offset, camera.kind, region=batch)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            self.trace(scenes, [cam], results, stream=st)
+            e1.record(st)
+            progress.submitted(batch)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            progress.completed(ms)
+            done.append((batch, ms))
+        return results, done
 
     def refine_shadow_edges(self, scenes, cameras, primary: TraceResults, stream=None):
         """Coverage per result slot after glc_trace of the same job into `primary`: 1 escape, 0 capture,

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define GLC_ABI_VERSION 2
+#define GLC_ABI_VERSION 3
 
 typedef enum glc_status {
   GLC_OK = 0,
@@ -165,6 +165,12 @@ typedef struct glc_policy {
                                      cameras of surface-free scenes; certified rays skip integration */
   uint32_t escape_map;            /* 1: escape-direction map (node pass on every 4th pixel, stable
                                      8x8 tiles of surface-free scenes reconstructed by interpolation) */
+  uint32_t mixed_split;           /* MIXED with persistent = 0: 1 (default) two kernels, binary32
+                                     stepping with the pair state until a ray's first step that
+                                     brackets a terminal event or enters the shell, then binary64
+                                     from a 128-byte hand-off record per ray (context memory,
+                                     grow-only); 0: one kernel whose warps step in binary64 while
+                                     a lane is inside the shell */
 } glc_policy;
 
 typedef enum glc_camera_kind {
@@ -182,6 +188,14 @@ typedef struct glc_camera {
   uint64_t n_rays;                /* RAYLIST: number of rays (images: ignored) */
   double affine_direction;        /* RAYLIST: +1 or -1 (images trace backward, -1) */
   uint64_t result_offset;         /* first result slot of this camera */
+  /* Image cameras: the batch of 8x8-pixel tiles to trace, as TileRegion { origin, workgroups }
+   * (crates/gravlume-render/src/trace.rs:799-857) with TRACE_WORKGROUP_AXIS = 8. tile_count {0, 0}
+   * traces the whole view. Results keep the whole view's layout (slot result_offset + y * width +
+   * x), and only the batch's pixels are written, so a frame traced batch by batch equals the
+   * frame traced at once. Accepted by glc_trace, glc_trace_host, glc_graph_capture and
+   * glc_trace_static_scratch; the shadow-edge, footprint and adjoint passes take whole views. */
+  uint32_t tile_origin[2];        /* first tile (column, row) */
+  uint32_t tile_count[2];         /* tiles (columns, rows), within the view's tile grid */
 } glc_camera;
 
 /* Caller-owned device SoA, one 16-byte element per ray in each array (128-bit stores). Any
@@ -384,12 +398,16 @@ glc_status glc_tape_destroy(glc_tape* tape);
 /* ---- trace without device allocation ------------------------------------------------------ */
 /* No counterpart in the reference: its wgpu trace pass always allocates its own target and
  * scratch. For callers that may not allocate device memory (a host whose frame allocator owns the
- * device heap, a plugin confined to buffers its host hands it): the persistent work-queue trace of
- * glc_trace, without a context. Its scratch (queue counter and job table) is a 96 KiB static
- * device array, so at most 128 scenes and 128 cameras (GLC_ERR_CAPACITY beyond). Runs on the
- * current device; the first call on a device looks up the array's address, so make it before any
- * stream capture. All calls share the array: calls that overlap on the GPU race. Scenes, cameras
- * and policy are host structs; results (and RAYLIST states) are device pointers. */
+ * device heap, a plugin confined to buffers its host hands it): the trace of glc_trace, without a
+ * context. Its scratch (queue counter and job table) is a 96 KiB static device array, so at most
+ * 128 scenes and 128 cameras (GLC_ERR_CAPACITY beyond). Runs on the current device; the first
+ * call on a device looks up the array's address, so make it before any stream capture (a
+ * cudaDeviceReset makes the next call look it up again). All calls share the array: calls that
+ * overlap on the GPU race. Scenes, cameras and policy are host structs; results (and RAYLIST
+ * states) are device pointers. The policy is checked as by glc_set_policy; `persistent` picks the
+ * kernel as in glc_trace; MIXED always runs as one kernel (mixed_split is ignored: the two-kernel
+ * form needs a hand-off record per ray); capture_certificates and escape_map must be 0
+ * (GLC_ERR_INVALID_ARGUMENT otherwise). Tile regions are accepted. */
 glc_status glc_trace_static_scratch(const glc_scene* scenes, int32_t n_scenes, const glc_camera* cameras,
                                     int32_t n_cameras, const glc_policy* policy, const glc_results* out,
                                     void* stream);

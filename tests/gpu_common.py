@@ -70,6 +70,10 @@ def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
             rep["event_residual_gpu_max"] = float(np.nanmax(gpu["event_residual"][sel][ev]))
         for k in ("max_null_residual", "max_lz_drift", "max_carter_drift"):
             rep[k] = float(np.max(np.abs(gpu[k][sel][same] - ref[same, F[k]])))
+        if "max_energy_drift" in gpu:
+            # E = -p_t is a constant of the stationary metric's Hamiltonian flow in both: zero drift
+            rep["max_energy_drift"] = float(np.max(np.abs(gpu["max_energy_drift"][sel][same] -
+                                                          ref[same, F["max_energy_drift"]])))
         rep["radial_turnings_mismatch"] = int((gpu["radial_turnings"][sel][same] != ref[same, F["radial_turnings"]]).sum())
         rep["equatorial_crossings_mismatch"] = int(
             (gpu["equatorial_crossings"][sel][same] != ref[same, F["equatorial_crossings"]]).sum())

@@ -51,6 +51,21 @@ def trace_states(scene, policy, states, direction):
     return d
 
 
+def trace_split(scene, policy, states, direction):
+    """MIXED as two kernels: the binary32 bulk stepper until its hand-off, the 128-byte hand-off
+    record, then the binary64 completion (the device kernels' per-ray logic, compiled for the host)."""
+    st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+    out = np.zeros((st.shape[0], len(FIELDS)))
+    f = lib().host_trace_split
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_double,
+                  ctypes.c_void_p]
+    assert f(ctypes.byref(scene), ctypes.byref(policy), st.shape[0], st.ctypes.data, direction,
+             out.ctypes.data) == 0
+    d = {k: out[:, i] for i, k in enumerate(FIELDS)}
+    d["termination"] = d["termination"].astype(int)
+    return d
+
+
 def adjoint_states(scene, policy, states, direction, dl_dobs):
     """Per ray: dL/d(x, y, z, p_x, p_y, p_z) at the initial state, dL/dE, dL/da, dL/dQ^2,
     termination, ok flag, accepted steps (the device adjoint's sweeps, compiled for the host)."""

@@ -51,9 +51,66 @@ void run(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st
     o[28] = ray.f64steps;
   }
 }
+// MIXED as two kernels: BULK steps each ray until it hands off, the record is packed and unpacked
+// as between the kernels, and TAIL finishes the ray (the outputs are TAIL's).
+void run_split(const glc_scene& sc, const glc_policy& pol, int64_t n, const double* st, double dir, double* out,
+               int nf) {
+  const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor);
+  for (int64_t i = 0; i < n; ++i) {
+    Ray<kBULK> bulk;
+    bulk.init(ls, pol, st + 8 * i, dir);
+    RayResult<float> bres;
+    while (!bulk.step(ls, pol, bres, false)) {
+    }
+    HandoffRec rec;
+    handoff_pack(bulk, bres, rec);
+    Ray<kTAIL> ray;
+    uint32_t failure = 0;
+    const uint32_t term = handoff_unpack(rec, ray, ls, st + 8 * i, dir, failure);
+    RayResult<double> res;
+    if (term != GLC_TERM_NONE) {
+      ray.finish_plain(res, term, failure);
+    } else {
+      while (!ray.step(ls, pol, res, false)) {
+      }
+    }
+    double* o = out + nf * i;
+    o[0] = res.termination;
+    o[1] = res.failure;
+    o[2] = res.candidates;
+    o[3] = res.flags;
+    o[4] = ray.accepted;
+    o[5] = ray.rejected;
+    o[6] = ray.turnings;
+    o[7] = ray.crossings;
+    o[8] = ray.winding;
+    o[9] = res.escape_theta;
+    o[10] = res.escape_phi;
+    o[11] = res.surface_r;
+    o[12] = res.surface_phi;
+    o[13] = res.g;
+    o[14] = ray.travel();
+    o[15] = res.event_residual;
+    o[16] = ray.affine();
+    o[17] = ray.dnull;
+    o[18] = ray.dlz;
+    o[19] = ray.dq;
+    o[20] = ray.turn_r;
+    o[21] = ray.azimuth_advance();
+    for (int c = 0; c < 6; ++c) o[22 + c] = ray.ys(c);
+    o[28] = ray.f64steps;
+  }
+}
 }  // namespace
 
 extern "C" int host_trace_fields() { return 29; }
+
+// precision 0 FP32, 1 MIXED (one kernel), 2 FP64, 3 MIXED as two kernels (BULK + TAIL)
+extern "C" int host_trace_split(const glc_scene* sc, const glc_policy* pol, int64_t n, const double* states,
+                                double dir, double* out) {
+  run_split(*sc, *pol, n, states, dir, out, 29);
+  return 0;
+}
 
 extern "C" int host_trace_states(const glc_scene* sc, const glc_policy* pol, int64_t n, const double* states,
                                  double dir, double* out) {

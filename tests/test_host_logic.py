@@ -56,6 +56,35 @@ def test_mixed_errors_are_below_plain_fp32(config1_rays):
     assert m["event_residual_gpu_max"] <= 1e-3 * f["event_residual_gpu_max"]
 
 
+def test_split_mixed_matches_the_oracle(config1_rays):
+    """MIXED as two kernels (binary32 bulk stepping, hand-off record, binary64 completion): the
+    same classes, turning points and crossings as the oracle, the one-kernel MIXED budgets, and a
+    binary64 event residual."""
+    sc, states, ref = config1_rays
+    d = H.trace_split(sc, G.ReferencePolicy.frame(G.Precision.MIXED), states, -1.0)
+    rep = compare(d, np.arange(len(states)), ref)
+    assert rep["class_mismatch"] == 0, rep
+    assert rep["radial_turnings_mismatch"] == 0 and rep["equatorial_crossings_mismatch"] == 0, rep
+    for k, tol in BUDGETS[G.Precision.MIXED].items():
+        assert rep[k] <= tol, (k, rep)
+    assert rep["event_residual_gpu_max"] <= 1e-9, rep
+    # every ray was finished by the binary64 completion (at least the re-taken terminal step)
+    assert (d["f64_steps"] >= 1).all()
+
+
+def test_split_mixed_equals_one_kernel_mixed_before_the_hand_off(config1_rays):
+    """Both MIXED forms step the same binary32 pair state, so they agree to a few binary32 ulps of
+    the rtol 1e-6 truncation error on every observable and take the same number of accepted steps
+    within the re-taken terminal step."""
+    sc, states, ref = config1_rays
+    pol = G.ReferencePolicy.frame(G.Precision.MIXED)
+    a = H.trace_split(sc, pol, states, -1.0)
+    b = H.trace_states(sc, pol, states, -1.0)
+    assert (a["termination"] == b["termination"]).all()
+    assert np.all(np.abs(a["accepted_steps"] - b["accepted_steps"]) <= 2)
+    assert np.nanmax(np.abs(a["travel_time"] - b["travel_time"])) < 1e-3
+
+
 def test_escape_is_never_lost_across_precisions():
     """A ray leaving the escape sphere must terminate there in every mode (no step exhaustion)."""
     obs = config1_observation(width=64, height=64)
