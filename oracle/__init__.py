@@ -426,3 +426,22 @@ def ind_gradients(mass, spin, charge, chart, policy, ev, states, direction=-1.0,
         raise ValueError(f"spacetime rejected ({rc})")
     return {"termination": out[:, 0].astype(int), "ok": out[:, 1] == 1.0, "obs": out[:, 2:6],
             "grad": out[:, 6:].reshape(n, 6, 4)}
+
+
+def variational_gradients(mass, spin, charge, chart, policy, ev, states, direction=-1.0, threads=1):
+    """Variational-equation reference gradients (forward-mode sensitivities of the oracle's own
+    trace, replayed on its accepted steps, with the implicit-function rule for the event time), in
+    the layout of ind_gradients: termination, ok, the 4 observables IND_OBS and d(observables)/d(param)
+    for IND_PARAMS."""
+    states = _c(states, np.float64).reshape(-1, 8)
+    n = states.shape[0]
+    out = np.zeros((n, 30))
+    f = lib().gro_variational_gradients
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+    rc = f(mass, spin, charge, chart, ctypes.byref(policy), ctypes.byref(ev), n, states.ctypes.data, direction,
+           threads, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"spacetime rejected ({rc})")
+    return {"termination": out[:, 0].astype(int), "ok": out[:, 1] == 1.0, "obs": out[:, 2:6],
+            "grad": out[:, 6:].reshape(n, 6, 4)}

@@ -14,6 +14,7 @@
 #include "oracle_footprint.hpp"
 #include "oracle_radiation.hpp"
 #include "oracle_tracer.hpp"
+#include "oracle_variational.hpp"
 #include "oracle_wgsl_rk4.hpp"
 
 using namespace gro;
@@ -441,6 +442,28 @@ int gro_ind_gradients(double m, double a, double q, int chart, const gro_policy*
       }
     }
     row[1] = 1.0;
+  });
+  return 0;
+}
+
+// Variational-equation reference gradients (oracle_variational.hpp): per ray (termination, ok, the
+// 4 observables of gro_ind_gradients, then their derivatives with respect to (p_t, p_x, p_y, p_z,
+// a, Q), param-major), the same 30-column layout as gro_ind_gradients.
+int gro_variational_gradients(double m, double a, double q, int chart, const gro_policy* pol, const gro_events* ev,
+                              int64_t n, const double* states, double direction, int threads, double* out) {
+  Spacetime sp;
+  if (!Spacetime::make(m, a, q, chart ? Chart::Outgoing : Chart::Ingoing, sp)) return -100;
+  const Tracer base{sp, to_policy(*pol), to_events(*ev)};
+  parallel_for(n, threads, [&](int64_t i) {
+    double* row = out + 30 * i;
+    Termination term;
+    double obs[4], grad[kVarParams][4];
+    const bool ok = variational_gradient(base, states + 8 * i, direction, term, obs, grad);
+    row[0] = double(int(term));
+    row[1] = ok ? 1.0 : 0.0;
+    for (int k = 0; k < 4; ++k) row[2 + k] = obs[k];
+    for (int p = 0; p < kVarParams; ++p)
+      for (int k = 0; k < 4; ++k) row[6 + 4 * p + k] = ok ? grad[p][k] : 0.0;
   });
   return 0;
 }

@@ -227,6 +227,7 @@ struct Outcome {
   int event_kind;             // -1 when the terminal has no localized event
   uint32_t event_candidates;  // bit k set: event kind k within tie tolerance
   double event_affine, event_bracket, event_residual;
+  double event_theta;         // fraction of the terminal step at the event (the variational reference reads it)
   double state[8];
   double affine_parameter;
   bool has_turning_radius;
@@ -623,6 +624,7 @@ inline Outcome Tracer::trace(const double initial[8], double sign, std::vector<d
       o.event_affine = std::fma(step, r.theta, affine);
       o.event_bracket = r.bracket;
       o.event_residual = r.residual;
+      o.event_theta = r.theta;
       Termination term = Termination::HorizonCrossing;
       switch (r.kind) {
         case kSingularity: term = Termination::SingularityGuard; break;
