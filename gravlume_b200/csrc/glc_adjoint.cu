@@ -32,34 +32,56 @@ __device__ __noinline__ bool adjoint_step(Ray<P>& ray, const LaneScene& ls, cons
   return ray.step(ls, pol, res, use64);
 }
 
-// Checkpoint c of ray gi: the ray object as 16-byte words, word-major across rays (coalesced).
+// Checkpoint storage: the ray object as 16-byte words. The first `cap` checkpoints of every ray
+// sit in the dense region, word-major across rays (coalesced); a ray that takes more keeps the rest
+// in the overflow pool, contiguously from its own base slot (sized by the rays' actual counts).
+struct CkptStore {
+  uint4* dense;
+  uint4* pool;
+  uint32_t cap;
+  unsigned long long n;
+};
+
 template <int P>
-__device__ __forceinline__ void store_ray(const Ray<P>& ray, uint4* ckpt, uint32_t c, unsigned long long n,
+__device__ __forceinline__ uint4* ckpt_word(const CkptStore& cs, uint32_t c, uint32_t base, unsigned long long gi,
+                                            int w) {
+  constexpr int W = RayWords<P>::kWords;
+  if (c < cs.cap) return cs.dense + ((unsigned long long)c * W + w) * cs.n + gi;
+  return cs.pool + ((unsigned long long)base + (c - cs.cap)) * W + w;
+}
+
+template <int P>
+__device__ __forceinline__ void store_ray(const Ray<P>& ray, const CkptStore& cs, uint32_t c, uint32_t base,
                                           unsigned long long gi) {
   constexpr int W = RayWords<P>::kWords;
   uint4 buf[W];
   memcpy(buf, &ray, sizeof(Ray<P>));
 #pragma unroll
-  for (int w = 0; w < W; ++w) ckpt[((unsigned long long)c * W + w) * n + gi] = buf[w];
+  for (int w = 0; w < W; ++w) *ckpt_word<P>(cs, c, base, gi, w) = buf[w];
 }
 
 template <int P>
-__device__ __forceinline__ void load_ray(Ray<P>& ray, const uint4* ckpt, uint32_t c, unsigned long long n,
+__device__ __forceinline__ void load_ray(Ray<P>& ray, const CkptStore& cs, uint32_t c, uint32_t base,
                                          unsigned long long gi) {
   constexpr int W = RayWords<P>::kWords;
   uint4 buf[W];
 #pragma unroll
-  for (int w = 0; w < W; ++w) buf[w] = ckpt[((unsigned long long)c * W + w) * n + gi];
+  for (int w = 0; w < W; ++w) buf[w] = *ckpt_word<P>(cs, c, base, gi, w);
   memcpy(&ray, buf, sizeof(Ray<P>));
 }
 
-// meta per ray: x checkpoints taken, y termination, z accepted steps, w 1 traced / 2 checkpoint
-// capacity exceeded / 0 tile padding. counters: [0] rays over capacity, [1] most accepted steps,
-// [2] replay mismatches, [3] degenerate terminal events.
+// meta per ray: x checkpoints taken, y termination | status << 8 (status 1 every checkpoint stored,
+// 2 waiting for its overflow slots, 0 tile padding), z accepted steps, w base slot in the overflow
+// pool. counters: [0] rays over the dense capacity, [1] most accepted steps, [2] replay mismatches,
+// [3] degenerate terminal events, [4] overflow slots reserved.
+//
+// pass 0 traces every ray, stores its first cs.cap checkpoints and reserves overflow slots for the
+// rest; pass 1 (only when some ray overflowed, after the pool is sized) traces the overflowing rays
+// again, bitwise identically, and stores their remaining checkpoints.
 template <int P>
 __global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_policy pol, glc_results out,
-                                                              uint32_t K, uint32_t cap, uint4* ckpt, uint4* meta,
-                                                              unsigned int* counters) {
+                                                              uint32_t K, CkptStore cs, uint4* meta,
+                                                              unsigned int* counters, int pass) {
   using S = typename PrecTraits<P>::S;
   const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= job.total) return;
@@ -67,6 +89,12 @@ __global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_p
   unsigned long long slot;
   int scene_idx, shortcut;
   double rdir[3];
+  uint32_t base = 0;
+  if (pass == 1) {
+    const uint4 m = meta[gi];
+    if ((m.y >> 8) != 2u) return;
+    base = m.w;
+  }
   if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) {
     meta[gi] = make_uint4(0, 0, 0, 0);
     return;
@@ -76,34 +104,40 @@ __global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_p
   ray.init(ls, pol, st8, dir);
   RayResult<S> res;
   uint32_t taken = 0;
-  bool over = false;
   for (;;) {
     if (ray.accepted == taken * K) {
-      if (taken < cap) store_ray<P>(ray, ckpt, taken, job.total, gi);
-      else over = true;
+      if (pass == 0 ? taken < cs.cap : taken >= cs.cap) store_ray<P>(ray, cs, taken, base, gi);
       ++taken;
     }
     if (adjoint_step<P>(ray, ls, pol, res)) break;
   }
+  if (pass == 1) {
+    meta[gi].y = res.termination | (1u << 8);
+    return;
+  }
   write_result<P>(out, slot, ray, res, ls);
-  meta[gi] = make_uint4(taken, res.termination, ray.accepted, over ? 2u : 1u);
-  if (over) atomicAdd(counters, 1u);
+  const bool over = taken > cs.cap;
+  if (over) {
+    atomicAdd(counters, 1u);
+    base = atomicAdd(counters + 4, taken - cs.cap);
+  }
+  meta[gi] = make_uint4(taken, res.termination | ((over ? 2u : 1u) << 8), ray.accepted, base);
   atomicMax(counters + 1, ray.accepted);
 }
 
-// Adjoint of every ray: replay each checkpointed segment (recording the start state and step size
-// of each attempt in scratch, K entries per ray) and sweep it in reverse, last segment first.
+// Adjoint of one ray: replay each checkpointed segment (recording the start state and step size of
+// each attempt in the thread's scratch, K entries) and sweep it in reverse, last segment first.
 template <int P>
-__global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K,
-                                                               const uint4* ckpt, const uint4* meta, double* scratch,
-                                                               const double* dl, glc_grads g, const double* dconst,
-                                                               double charge, unsigned int* counters) {
+__device__ void adjoint_backward_ray(const JobView& job, const glc_policy& pol, uint32_t K, const CkptStore& cs,
+                                     const uint4* meta, double* scratch, unsigned long long stride,
+                                     unsigned long long gi, const double* dl, const glc_grads& g,
+                                     const double* dconst, double charge, unsigned int* counters) {
   using S = typename PrecTraits<P>::S;
-  const unsigned long long n = job.total;
-  const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gi >= n) return;
-  const uint4 m = meta[gi];
-  if (m.w == 0u) return;
+  const unsigned long long n = stride;
+  uint4 m = meta[gi];
+  const uint32_t status = m.y >> 8;
+  m.y &= 0xFFu;
+  if (status == 0u) return;
   double st8[8], dir;
   unsigned long long slot;
   int scene_idx, shortcut;
@@ -121,14 +155,14 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
     any = any || wobs[k] != 0.0;
   }
   double lam[6] = {0, 0, 0, 0, 0, 0}, gacc[3] = {0, 0, 0};
-  const bool differentiable = m.w == 1u && (m.y == GLC_TERM_SURFACE || m.y == GLC_TERM_ESCAPE);
+  const bool differentiable = status == 1u && (m.y == GLC_TERM_SURFACE || m.y == GLC_TERM_ESCAPE);
   bool ok = differentiable && any;
   bool degenerate = false;
   double wst[7];
   step_weights(wst);
   for (int c = int(m.x) - 1; ok && c >= 0; --c) {
     Ray<P> ray;
-    load_ray<P>(ray, ckpt, uint32_t(c), n, gi);
+    load_ray<P>(ray, cs, uint32_t(c), m.w, gi);
     RayResult<S> res;
     uint32_t j = 0;
     bool term = false;
@@ -137,7 +171,7 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
         ok = false;
         break;
       }
-      double* rec = scratch + (unsigned long long)j * 7 * n + gi;
+      double* rec = scratch + (unsigned long long)j * 7 * n;
       for (int q = 0; q < 6; ++q) rec[q * n] = double(ray.ys(q));
       rec[6 * n] = double(ray.h);
       const uint32_t acc = ray.accepted;
@@ -158,7 +192,7 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
         ok = false;
         break;
       }
-      const double* rec = scratch + (unsigned long long)j * 7 * n + gi;
+      const double* rec = scratch + (unsigned long long)j * 7 * n;
       double y0[6];
       for (int q = 0; q < 6; ++q) y0[q] = rec[q * n];
       if (!terminal_reverse(ls, y0, E, rec[6 * n], double(res.event_theta), double(ray.dir), m.y, wobs, lam, gacc)) {
@@ -171,7 +205,7 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
       break;
     }
     for (int jj = int(j) - 1; jj >= 0; --jj) {
-      const double* rec = scratch + (unsigned long long)jj * 7 * n + gi;
+      const double* rec = scratch + (unsigned long long)jj * 7 * n;
       double y0[6], l0[6];
       for (int q = 0; q < 6; ++q) y0[q] = rec[q * n];
       dp5_reverse(ls.kn, kd, y0, E, rec[6 * n], wst, lam, l0, gacc);
@@ -220,6 +254,20 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
       if (pg[k] != 0.0) atomicAdd(g.params + k, pg[k]);
 }
 
+// Grid-stride over the rays: each thread's replay scratch (K attempts of 7 doubles, word-major
+// across the grid's threads) is reused for every ray it takes, so the scratch is bounded by the
+// grid, not by the ray count.
+template <int P>
+__global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K, CkptStore cs,
+                                                               const uint4* meta, double* scratch, const double* dl,
+                                                               glc_grads g, const double* dconst, double charge,
+                                                               unsigned int* counters) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (unsigned long long gi = tid; gi < job.total; gi += stride)
+    adjoint_backward_ray<P>(job, pol, K, cs, meta, scratch + tid, stride, gi, dl, g, dconst, charge, counters);
+}
+
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 void oblate_position(double spin, int chart, double r, double polar, double azimuth, double out[4]) {
@@ -252,8 +300,10 @@ struct glc_tape {
   double charge = 0.0;
   unsigned char* d_job = nullptr;
   size_t off_cams = 0, off_begin = 0, off_cert = 0;
-  uint4* d_ckpt = nullptr;
+  uint4* d_ckpt = nullptr;              // dense checkpoints: cap per ray, word-major across rays
   size_t ckpt_bytes = 0, ckpt_alloc = 0;
+  uint4* d_pool = nullptr;              // overflow checkpoints, sized by the rays' actual counts
+  size_t pool_bytes = 0, pool_alloc = 0;
   uint4* d_meta = nullptr;
   unsigned long long meta_alloc = 0;
   double* d_dconst = nullptr;
@@ -284,6 +334,7 @@ void free_tape(glc_tape* t) {
   if (!t) return;
   if (t->d_job) cudaFree(t->d_job);
   if (t->d_ckpt) cudaFree(t->d_ckpt);
+  if (t->d_pool) cudaFree(t->d_pool);
   if (t->d_meta) cudaFree(t->d_meta);
   if (t->d_dconst) cudaFree(t->d_dconst);
   if (t->d_scratch) cudaFree(t->d_scratch);
@@ -295,33 +346,44 @@ glc_status cuda_status(cudaError_t e) {
   return e == cudaSuccess ? GLC_OK : set_error(GLC_ERR_CUDA, cudaGetErrorString(e));
 }
 
+constexpr int kCounters = 8;
+
+CkptStore ckpt_store(const glc_tape* t) { return CkptStore{t->d_ckpt, t->d_pool, t->cap, t->n}; }
+
 template <int P>
-glc_status run_forward(glc_tape* t, const glc_results& out, cudaStream_t st) {
+glc_status run_forward(glc_tape* t, const glc_results& out, cudaStream_t st, int pass) {
   const unsigned grid = unsigned((t->n + 127) / 128);
-  glc_status s = cuda_status(cudaMemsetAsync(t->d_counters, 0, 4 * sizeof(unsigned int), st));
+  glc_status s = GLC_OK;
+  if (pass == 0) s = cuda_status(cudaMemsetAsync(t->d_counters, 0, kCounters * sizeof(unsigned int), st));
   if (s != GLC_OK) return s;
-  adjoint_forward_kernel<P><<<grid, 128, 0, st>>>(t->job(), t->pol, out, t->K, t->cap, t->d_ckpt, t->d_meta,
-                                                   t->d_counters);
+  adjoint_forward_kernel<P><<<grid, 128, 0, st>>>(t->job(), t->pol, out, t->K, ckpt_store(t), t->d_meta,
+                                                   t->d_counters, pass);
   s = cuda_status(cudaGetLastError());
   if (s == GLC_OK) t->ctx->stats.kernel_launches += 1;
   return s;
 }
 
-glc_status forward(glc_tape* t, const glc_results& out, cudaStream_t st) {
-  return t->pol.precision == GLC_MIXED ? run_forward<kMIXED>(t, out, st) : run_forward<kFP64>(t, out, st);
+glc_status forward(glc_tape* t, const glc_results& out, cudaStream_t st, int pass) {
+  return t->pol.precision == GLC_MIXED ? run_forward<kMIXED>(t, out, st, pass) : run_forward<kFP64>(t, out, st, pass);
 }
 
-// Checkpoint slots for every ray; the allocation only grows (a reused tape keeps its memory).
-glc_status size_checkpoints(glc_tape* t, uint32_t cap) {
-  t->cap = cap;
-  t->ckpt_bytes = size_t(cap) * t->words * 16 * t->n;
-  if (t->ckpt_bytes <= t->ckpt_alloc) return GLC_OK;
-  if (t->d_ckpt) cudaFree(t->d_ckpt);
-  t->d_ckpt = nullptr;
-  t->ckpt_alloc = 0;
-  const glc_status s = cuda_status(cudaMalloc(&t->d_ckpt, t->ckpt_bytes));
-  if (s == GLC_OK) t->ckpt_alloc = t->ckpt_bytes;
+// A grow-only device buffer of the tape (a reused tape keeps its memory).
+glc_status grow(uint4** buf, size_t* alloc, size_t need) {
+  if (need <= *alloc) return GLC_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *alloc = 0;
+  const glc_status s = cuda_status(cudaMalloc(buf, need));
+  if (s == GLC_OK) *alloc = need;
   return s;
+}
+
+// Dense checkpoint slots for every ray: the checkpoints of the first 64 accepted steps (every ray
+// takes at least its initial one); the rest go to the overflow pool.
+glc_status size_checkpoints(glc_tape* t) {
+  t->cap = 64 / t->K + 1;
+  t->ckpt_bytes = size_t(t->cap) * t->words * 16 * t->n;
+  return grow(&t->d_ckpt, &t->ckpt_alloc, t->ckpt_bytes);
 }
 
 struct DeviceScope {
@@ -424,24 +486,25 @@ glc_status fill_tape(glc_tape* t, glc_ctx* ctx, const glc_adjoint_scene* as, con
   }
   if ((!t->d_job && cudaMalloc(&t->d_job, job_bytes) != cudaSuccess) ||
       (!t->d_dconst && cudaMalloc(&t->d_dconst, sizeof(dconst)) != cudaSuccess) ||
-      (!t->d_counters && cudaMalloc(&t->d_counters, 4 * sizeof(unsigned int)) != cudaSuccess))
+      (!t->d_counters && cudaMalloc(&t->d_counters, kCounters * sizeof(unsigned int)) != cudaSuccess))
     return set_error(GLC_ERR_CUDA, "tape allocation failed");
   // pageable sources: both copies have consumed their bytes when they return
   if (cudaMemcpyAsync(t->d_job, host_job, job_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(t->d_dconst, dconst, sizeof(dconst), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return set_error(GLC_ERR_CUDA, "tape upload failed");
-  // checkpoint slots for 512 accepted steps; when a ray needs more, the pass runs again with the
-  // capacity its longest ray needs
-  s = size_checkpoints(t, uint32_t(512 / t->K + 2));
-  if (s == GLC_OK) s = forward(t, *out, st);
+  // pass 0: every ray, its first checkpoints in the dense slots, overflow slots reserved for the rest;
+  // pass 1 (when some ray overflowed): those rays again, into the pool sized by their counts
+  s = size_checkpoints(t);
+  if (s == GLC_OK) s = forward(t, *out, st, 0);
   if (s != GLC_OK) return s;
-  unsigned int counters[4];
+  unsigned int counters[kCounters];
   if (cudaMemcpyAsync(counters, t->d_counters, sizeof(counters), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return set_error(GLC_ERR_CUDA, "forward pass failed");
+  t->pool_bytes = size_t(counters[4]) * t->words * 16;
   if (counters[0] > 0) {
-    s = size_checkpoints(t, counters[1] / t->K + 2);
-    if (s == GLC_OK) s = forward(t, *out, st);
+    s = grow(&t->d_pool, &t->pool_alloc, t->pool_bytes);
+    if (s == GLC_OK) s = forward(t, *out, st, 1);
     if (s != GLC_OK) return s;
   }
   return GLC_OK;
@@ -482,7 +545,16 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
   if (!t || !dl || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
   if (!t->valid) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape's last forward pass failed; run it again");
   DeviceScope scope(t->ctx->device);
-  const size_t need = size_t(t->K) * 7 * sizeof(double) * t->n;
+  // a grid of the SMs times the kernel's occupancy; each thread keeps K attempts of 7 doubles
+  int per_sm = 0;
+  glc_status s0 = cuda_status(t->pol.precision == GLC_MIXED
+                                  ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kMIXED>, 128, 0)
+                                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kFP64>, 128, 0));
+  if (s0 != GLC_OK) return s0;
+  unsigned long long grid = (unsigned long long)t->ctx->sm_count * (per_sm > 0 ? per_sm : 1);
+  const unsigned long long grid_cap = (t->n + 127) / 128;
+  if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
+  const size_t need = size_t(t->K) * 7 * sizeof(double) * grid * 128;
   if (need > t->scratch_bytes) {
     if (t->d_scratch) cudaFree(t->d_scratch);
     t->d_scratch = nullptr;
@@ -492,14 +564,15 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
     t->scratch_bytes = need;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const unsigned grid = unsigned((t->n + 127) / 128);
   const double* dconst = t->pinhole ? t->d_dconst : nullptr;
   if (t->pol.precision == GLC_MIXED)
-    adjoint_backward_kernel<kMIXED><<<grid, 128, 0, st>>>(t->job(), t->pol, t->K, t->d_ckpt, t->d_meta, t->d_scratch,
-                                                          dl, *out, dconst, t->charge, t->d_counters);
+    adjoint_backward_kernel<kMIXED><<<unsigned(grid), 128, 0, st>>>(t->job(), t->pol, t->K, ckpt_store(t), t->d_meta,
+                                                                    t->d_scratch, dl, *out, dconst, t->charge,
+                                                                    t->d_counters);
   else
-    adjoint_backward_kernel<kFP64><<<grid, 128, 0, st>>>(t->job(), t->pol, t->K, t->d_ckpt, t->d_meta, t->d_scratch,
-                                                         dl, *out, dconst, t->charge, t->d_counters);
+    adjoint_backward_kernel<kFP64><<<unsigned(grid), 128, 0, st>>>(t->job(), t->pol, t->K, ckpt_store(t), t->d_meta,
+                                                                   t->d_scratch, dl, *out, dconst, t->charge,
+                                                                   t->d_counters);
   const glc_status s = cuda_status(cudaGetLastError());
   if (s == GLC_OK) t->ctx->stats.kernel_launches += 1;
   return s;
@@ -509,7 +582,7 @@ glc_status glc_tape_info(const glc_tape* t, uint64_t* rays, uint32_t* slots, uin
   if (!t) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
   if (rays) *rays = t->n;
   if (slots) *slots = t->cap;
-  if (bytes) *bytes = t->ckpt_bytes + t->scratch_bytes + t->n * sizeof(uint4);
+  if (bytes) *bytes = t->ckpt_bytes + t->pool_bytes + t->scratch_bytes + t->n * sizeof(uint4);
   return GLC_OK;
 }
 
