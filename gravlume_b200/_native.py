@@ -68,7 +68,8 @@ class Policy(ctypes.Structure):
         ("blocks_per_sm", c_uint32), ("tile_w", c_uint32), ("tile_h", c_uint32),
         ("refill_interval", c_uint32), ("rays_per_grab", c_uint32),
         ("refill_min_idle", c_uint32), ("mixed_pair_state", c_uint32), ("capture_certificates", c_uint32),
-        ("escape_map", c_uint32), ("mixed_split", c_uint32),
+        ("escape_map", c_uint32), ("mixed_split", c_uint32), ("uncertain_terminals", c_uint32),
+        ("uncertain_drift_limit", c_double),
     ]
 
     def as_dict(self):
@@ -117,6 +118,7 @@ SIGNATURES = {
     "glc_prograde_isco": (c_int32, [c_double, c_double, ctypes.POINTER(c_double)]),
     "glc_policy_default": (c_int32, [c_int32, c_int32, ctypes.POINTER(Policy)]),
     "glc_flop_model": (c_int32, [c_void_p]),
+    "glc_selftest_event_policy": (c_int32, [ctypes.POINTER(Policy), c_void_p, c_void_p]),
     "glc_rhs_host": (c_int32, [ctypes.POINTER(Scene), c_void_p, c_double, c_int32, c_void_p]),
     "glc_create": (c_int32, [c_int32, ctypes.POINTER(c_void_p)]),
     "glc_destroy": (c_int32, [c_void_p]),

@@ -29,6 +29,50 @@ glc_status set_error(glc_status status, const char* message) {
 }
 }  // namespace glc
 
+namespace glc {
+
+// The reference's synthetic event-policy cases (event_policy_capture.wgsl), evaluated by the trace
+// kernels' own earliest-event selection and arming test: one thread per case.
+template <int kCases>
+__global__ void event_policy_cases_kernel(glc_policy pol, uint32_t* out) {
+  const int c = int(threadIdx.x);
+  if (c >= kCases) return;
+  uint32_t r[4] = {0u, 0u, 0u, 0u};
+  const double tie = pol.event_tie_tolerance, band = pol.event_arming_band;
+  if (c < 4) {
+    int kinds[4];
+    double thetas[4];
+    int n = 0;
+    double step = 1.0;
+    if (c == 3) {
+      // horizon at one half, the surface 0.75 tie tolerances before it, the escape sphere as far after
+      const double off = 0.75 * tie / step;
+      kinds[n] = kEvHorizon, thetas[n++] = 0.5;
+      kinds[n] = kEvSurface, thetas[n++] = 0.5 - off;
+      kinds[n] = kEvEscape, thetas[n++] = 0.5 + off;
+    } else {
+      // escape sphere at one half; the surface half a tie tolerance later (cases 0 and 1, at the
+      // largest and the smallest step) or at the same fraction (case 2)
+      step = c == 0 ? pol.maximum_step : pol.minimum_step;
+      kinds[n] = kEvSurface, thetas[n++] = c < 2 ? 0.5 + 0.5 * tie / step : 0.5;
+      kinds[n] = kEvEscape, thetas[n++] = 0.5;
+    }
+    uint32_t cand = 0;
+    const int first = earliest_event<double>(kinds, thetas, n, step, tie, cand);
+    r[0] = first >= 0 ? termination_of_event(kinds[first]) : 0u;
+    r[1] = cand;
+    r[2] = (cand & (cand - 1u)) != 0u ? 1u : 0u;
+  } else {
+    // surface arming: value 0, half the band, twice the band, and an event armed before
+    const double v = c == 5 ? 0.5 * band : (c == 6 ? 2.0 * band : 0.0);
+    const bool armed = c == 7 || event_clears_band<double>(kEvSurface, v, band);
+    r[0] = armed ? 1u : 0u;
+  }
+  reinterpret_cast<uint4*>(out)[c] = make_uint4(r[0], r[1], r[2], r[3]);
+}
+
+}  // namespace glc
+
 #define GLC_CUDA(expr)                                                                          \
   do {                                                                                          \
     cudaError_t e_ = (expr);                                                                    \
@@ -331,6 +375,8 @@ glc_status validate_policy(const glc_policy& p) {
     return set_error(GLC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 up to 128");
   if (p.tile_w == 0 || p.tile_h == 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "tile shape must be nonzero");
   if (p.persistent > 2) return set_error(GLC_ERR_INVALID_ARGUMENT, "unknown kernel choice (persistent 0, 1 or 2)");
+  if (p.uncertain_terminals > 1 || !(p.uncertain_drift_limit > 0.0))
+    return set_error(GLC_ERR_INVALID_ARGUMENT, "uncertain_terminals is 0 or 1 with a positive drift limit");
   return GLC_OK;
 }
 
@@ -539,7 +585,19 @@ glc_status glc_policy_default(int32_t preset, int32_t precision, glc_policy* out
   p.capture_certificates = 0;
   p.escape_map = 0;
   p.mixed_split = 1;
+  p.uncertain_terminals = 0;
+  p.uncertain_drift_limit = 0.05;
   *out = p;
+  return GLC_OK;
+}
+
+glc_status glc_selftest_event_policy(const glc_policy* policy, uint32_t* out, void* stream) {
+  if (!policy || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
+  if ((reinterpret_cast<uintptr_t>(out) & 15u) != 0) return set_error(GLC_ERR_INVALID_ARGUMENT, "out must be 16-byte aligned");
+  const glc_status s = validate_policy(*policy);
+  if (s != GLC_OK) return s;
+  event_policy_cases_kernel<8><<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(*policy, out);
+  GLC_CUDA(cudaGetLastError());
   return GLC_OK;
 }
 

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) escape_map_no
       const glc_scene& sc = job.scenes[cam.scene_index];
       double st8[8];
       image_state(&sc, &cam, px, py, st8);
-      const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, out.drift_a || out.drift_b);
+      const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
       Ray<P> ray;
       ray.init(ls, pol, st8, -1.0);
       RayResult<S> res;

@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) footprint_qua
       const glc_scene& sc = job.scenes[cam.scene_index];
       double st8[8];
       image_state(&sc, &cam, px, py, st8);
-      const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, false);  // no drift output
+      const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, pol.uncertain_terminals != 0u);  // drifts only for the Uncertain gate
       Ray<P> ray;
       ray.init(ls, pol, st8, -1.0);
       RayResult<S> res;
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(128, 2) footprint_tangent_kernel(
     const glc_scene& sc = job.scenes[cam.scene_index];
     double st8[8];
     image_state(&sc, &cam, px, py, st8);
-    const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, false);  // no drift output
+    const LaneScene ls = make_lane_scene(sc, pol.mixed_shell_factor, pol.uncertain_terminals != 0u);  // drifts only for the Uncertain gate
     Ray<P> ray;
     ray.init(ls, pol, st8, -1.0);
     RayResult<S> res;

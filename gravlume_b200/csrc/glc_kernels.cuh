@@ -394,7 +394,7 @@ __device__ __forceinline__ void trace_one(const JobView& job, const glc_policy& 
     return;
   }
   // the drift maxima are evaluated only when a drift array is wanted
-  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
   Ray<P> ray;
   ray.init(ls, pol, st8, dir);
   RayResult<S> res;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
     else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
     return;
   }
-  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
   Ray<kBULK> ray;
   ray.init(ls, pol, st8, dir);
   RayResult<float> res;
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
   double rdir[3];
   if (!ray_setup(job, pol, gi, st8, dir, slot, scene_idx, shortcut, rdir)) return;
   if (shortcut != kShortNone) return;
-  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+  const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
   Ray<kTAIL> ray;
   uint32_t failure = GLC_FAIL_NONE;
   const uint32_t term = handoff_resume(hv, gi, ray, ls, st8, dir, failure);
@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
               if (shortcut == kShortCertified) write_certified(out, slot);
               else if (shortcut == kShortReconstructed) write_reconstructed(out, slot, rdir);
             } else {
-              ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b);
+              ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
               ray.init(ls, pol, st8, dir);
               active = true;
             }

@@ -183,6 +183,26 @@ GLC_HD double event_scale(int kind, const LaneScene& sc) {
   }
 }
 
+// Earliest of n localized event roots (geodesic.rs:722-740): the smallest step fraction, the
+// first in kind order (guard, horizon, surface, escape) on equal fractions, and as candidate bits
+// every kind whose root lies within `tie` affine distance of it. Returns its index, -1 when n = 0.
+template <class T>
+GLC_HD int earliest_event(const int kinds[4], const T thetas[4], int n, T step_magnitude, T tie, uint32_t& cand) {
+  int first = -1;
+  for (int i = 0; i < n; ++i)
+    if (first < 0 || thetas[i] < thetas[first]) first = i;
+  cand = 0;
+  if (first >= 0)
+    for (int i = 0; i < n; ++i)
+      if (g_abs(thetas[i] - thetas[first]) * step_magnitude <= tie) cand |= 1u << kinds[i];
+  return first;
+}
+
+GLC_HD uint32_t termination_of_event(int kind) {
+  return kind == kEvGuard ? GLC_TERM_SINGULARITY
+                          : (kind == kEvSurface ? GLC_TERM_SURFACE : (kind == kEvEscape ? GLC_TERM_ESCAPE : GLC_TERM_HORIZON));
+}
+
 // Result of one ray, written by the tracer into the caller's SoA.
 template <class S>
 struct RayResult {
@@ -785,13 +805,8 @@ struct Ray {
         ++n;
       }
     }
-    int first = -1;
     uint32_t cand = 0;
-    for (int i = 0; i < n; ++i)
-      if (first < 0 || thetas[i] < thetas[first]) first = i;
-    if (first >= 0)
-      for (int i = 0; i < n; ++i)
-        if (g_abs(thetas[i] - thetas[first]) * g_abs(hh) <= T(pol.event_tie_tolerance)) cand |= 1u << kinds[i];
+    const int first = earliest_event<T>(kinds, thetas, n, g_abs(hh), T(pol.event_tie_tolerance), cand);
     const bool has_event = first >= 0;
     if (P == kBULK && has_event) {
       // a surface crossing at or near the surface: TAIL re-takes the step (not counted here)
@@ -799,6 +814,8 @@ struct Ray {
       return hand_off(res);
     }
     const T term_theta = has_event ? thetas[first] : T(1);
+    // the replaced GPU kernel's gate: the terminal inside a turning point's root bracket
+    bool turning_uncertain = false;
     // radial turning point (geodesic.rs:330-360)
     if ((o.mask >> 4) & 1u) {
       const T sv = T(dir * vr), evv = T(dir * o.vr_end);
@@ -810,7 +827,8 @@ struct Ray {
         v = T(dir * vv);
         return g_finite(v);
       };
-      if (localize(y, hh, dpoly, tol, sv, evv, vr_at, th_, yr, br) && (!has_event || th_ < term_theta)) {
+      const bool found = localize(y, hh, dpoly, tol, sv, evv, vr_at, th_, yr, br);
+      if (found && (!has_event || th_ < term_theta)) {
         turnings += 1;
         if (sv < T(0) && evv >= T(0)) {
           int gs;
@@ -818,6 +836,7 @@ struct Ray {
           if (gs == kGeomOk) turn_r = (turn_r == turn_r) ? C(g_min(T(turn_r), rr)) : C(rr);
         }
       }
+      if (has_event && (!found || g_abs(th_ - term_theta) * g_abs(hh) <= br)) turning_uncertain = true;
     }
     // equatorial crossing (geodesic.rs:362-383)
     if ((o.mask >> 5) & 1u) {
@@ -846,13 +865,14 @@ struct Ray {
     }
     add_affine_s(hh * term_theta);
     set_state(ycommit);
-    const int kind = kinds[first];
-    uint32_t term = GLC_TERM_HORIZON;
-    if (kind == kEvGuard) term = GLC_TERM_SINGULARITY;
-    else if (kind == kEvSurface) term = GLC_TERM_SURFACE;
-    else if (kind == kEvEscape) term = GLC_TERM_ESCAPE;
+    const uint32_t term = termination_of_event(kinds[first]);
     finish_event(sc, pol, res, term, cand, residuals[first], ycommit);
     res.event_theta = term_theta;
+    if (pol.uncertain_terminals) {
+      const double limit = pol.uncertain_drift_limit;
+      const bool drift = sc.track && (double(dnull) > limit || double(dlz) > limit || double(dq) > limit);
+      if ((cand & (cand - 1u)) != 0u || turning_uncertain || drift) res.termination = GLC_TERM_UNCERTAIN;
+    }
     return true;
   }
 

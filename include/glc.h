@@ -171,6 +171,16 @@ typedef struct glc_policy {
                                      from a 128-byte hand-off record per ray (context memory,
                                      grow-only); 0: one kernel whose warps step in binary64 while
                                      a lane is inside the shell */
+  uint32_t uncertain_terminals;   /* 1: the replaced wgpu kernel's gate (geodesic_integration.wgsl
+                                     324-330): a terminal becomes GLC_TERM_UNCERTAIN when more than
+                                     one event lies within the tie tolerance of the earliest, when
+                                     the terminal lies inside the bracket of a radial turning point
+                                     of its step, or when a recorded invariant drift exceeds
+                                     uncertain_drift_limit; 0 (default, the reference's CPU
+                                     semantics): the earliest event terminates and the tied kinds
+                                     are reported in the candidate bits of code.x */
+  double uncertain_drift_limit;   /* drift budget of the gate (INVARIANT_DRIFT_LIMIT 0.05,
+                                     crates/gravlume-render/src/trace/input.rs:13) */
 } glc_policy;
 
 typedef enum glc_camera_kind {
@@ -394,6 +404,17 @@ glc_status glc_backward(glc_tape* tape, const double* dL_dobs, const glc_grads* 
 /* Checkpoint sizing: rays traced, checkpoint slots per ray, device bytes held by the tape. */
 glc_status glc_tape_info(const glc_tape* tape, uint64_t* rays, uint32_t* slots_per_ray, uint64_t* bytes);
 glc_status glc_tape_destroy(glc_tape* tape);
+
+/* ---- test hook ----------------------------------------------------------------------------- */
+/* The event-policy cases of the reference's test-only capture pipeline
+ * (TracePipeline::for_event_policy_capture, crates/gravlume-render/src/gpu_capture.rs:145-150, and
+ * shaders/event_policy_capture.wgsl), run on the device by the same earliest-event selection and
+ * arming functions as the trace kernels, under `policy` (its tie tolerance, arming band and step
+ * limits). out: 16-byte aligned device array of 8 x 4 uint32. Cases 0-3: (termination, candidate
+ * bits, ambiguous, 0) of synthetic roots at fractions of the step; cases 4-7: (armed, 0, 0, 0) of
+ * the surface event for a value 0, half the band, twice the band, and an already armed event.
+ * Asynchronous on the stream. */
+glc_status glc_selftest_event_policy(const glc_policy* policy, uint32_t* out, void* stream);
 
 /* ---- trace without device allocation ------------------------------------------------------ */
 /* No counterpart in the reference: its wgpu trace pass always allocates its own target and

@@ -37,12 +37,20 @@ def pipe():
 
 @pytest.fixture(scope="module")
 def config1_oracle():
+    """Every pixel of the 256x256 frame by the oracle at rtol 1e-10 / atol 1e-12, and the
+    near-critical band: the pixels whose oracle class changes when its tolerance is loosened to
+    rtol 1e-7 / atol 1e-9 (their class is decided by less than the frame tolerance's truncation)."""
     obs = config1_observation()
     osc, ev, _ = oracle_for(obs)
-    px, py = seeded_pixels(256, 256, 240, seed=1)
-    ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=O.hardware_threads())
+    idx = np.arange(256 * 256)
+    px, py = idx % 256, idx // 256
+    threads = O.hardware_threads()
+    ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
     assert (status == 0).all()
-    return obs, py * 256 + px, ref
+    loose, _ = O.trace_pixels(osc, O.custom_policy(1e-7, 1e-9), ev, px, py, threads=threads)
+    band = ref[:, F["termination"]] != loose[:, F["termination"]]
+    assert band.sum() <= 0.005 * idx.size, int(band.sum())
+    return obs, idx, ref, band
 
 
 def run_image(pipe, obs, precision, **policy):
@@ -52,11 +60,11 @@ def run_image(pipe, obs, precision, **policy):
     return res.numpy()
 
 
-def test_fp64_image_matches_the_oracle_on_the_config1_sample(pipe, config1_oracle):
-    obs, sel, ref = config1_oracle
+def test_fp64_image_matches_the_oracle_on_every_config1_pixel(pipe, config1_oracle):
+    obs, sel, ref, band = config1_oracle
     d = run_image(pipe, obs, G.Precision.FP64)
-    rep = compare(d, sel, ref)
-    print("fp64", rep)
+    rep = compare(d, sel[~band], ref[~band])
+    print("fp64", rep, "band", int(band.sum()))
     assert rep["class_mismatch"] == 0, rep
     for k, tol in FP64_BUDGET.items():
         if k in rep:
@@ -65,15 +73,44 @@ def test_fp64_image_matches_the_oracle_on_the_config1_sample(pipe, config1_oracl
 
 
 @pytest.mark.parametrize("precision", [G.Precision.FP32, G.Precision.MIXED])
-def test_reduced_precision_images_stay_within_their_budgets(pipe, config1_oracle, precision):
-    obs, sel, ref = config1_oracle
+def test_reduced_precision_images_match_the_oracle_classes_outside_the_band(pipe, config1_oracle, precision):
+    obs, sel, ref, band = config1_oracle
     d = run_image(pipe, obs, precision)
-    rep = compare(d, sel, ref)
-    print(precision.name, rep)
-    assert rep["class_mismatch"] <= 0.02 * rep["n"], rep
+    rep = compare(d, sel[~band], ref[~band])
+    print(precision.name, rep, "band", int(band.sum()))
+    assert rep["class_mismatch"] == 0, rep
     for k, tol in F32_BUDGET.items():
         if k in rep:
             assert rep[k] <= tol, (k, rep)
+
+
+CONFIG2_SCENES = [(a, q, i) for a, q in ((0.0, 0.0), (0.5, 0.0), (0.9, 0.3), (0.998, 0.0), (0.6, 0.7))
+                  for i in (17.0, 60.0, 85.0)]
+
+
+@pytest.mark.parametrize("a,q,incl", CONFIG2_SCENES)
+def test_full_frame_scene_set_matches_the_oracle(pipe, a, q, incl):
+    """The full-frame precision set at 1920x1080: each of the 15 scenes in FP32, MIXED and FP64 at
+    the frame tolerance against 128 seeded oracle rays at rtol 1e-10; classes identical outside the
+    near-critical band (as for the 256x256 frame), observables within the frame budgets."""
+    w, h = 1920, 1080
+    obs = config1_observation(width=w, height=h, spin=a, charge=q, incl_deg=incl)
+    osc, ev, _ = oracle_for(obs)
+    px, py = seeded_pixels(w, h, 128, seed=int(1000 * a + 100 * q + incl))
+    threads = O.hardware_threads()
+    ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
+    assert (status == 0).all()
+    loose, _ = O.trace_pixels(osc, O.custom_policy(1e-7, 1e-9), ev, px, py, threads=threads)
+    band = ref[:, F["termination"]] != loose[:, F["termination"]]
+    sel = (py * w + px)[~band]
+    frame_tol = dict(position_rtol=1e-6, momentum_rtol=1e-6, position_atol=1e-8, momentum_atol=1e-8, maximum_step=1e3)
+    for precision, extra in ((G.Precision.FP32, {}), (G.Precision.MIXED, {}), (G.Precision.FP64, frame_tol)):
+        d = run_image(pipe, obs, precision, **extra)
+        rep = compare(d, sel, ref[~band])
+        assert rep["class_mismatch"] == 0, (precision.name, rep)
+        for k, tol in F32_BUDGET.items():
+            if k in rep:
+                assert rep[k] <= tol, (precision.name, k, rep)
 
 
 def test_persistent_and_simple_kernels_agree(pipe):
@@ -203,22 +240,16 @@ def test_full_hd_frame_never_exhausts_steps(pipe, precision):
 
 
 def test_mixed_is_at_or_below_plain_fp32_error_on_every_observable(pipe, config1_oracle):
-    """The precision study's acceptance at the same frame policy (rtol 1e-6), against the binary64
-    oracle. Both modes accept the same kind of step sequence, so observables set by the
-    controller's truncation error (directions, g, radii, travel time, invariant drifts) are the same
-    to within the scatter of a 240-ray maximum (a factor 1.5 plus one tolerance unit); what binary64
-    localization buys is
-    the event residual, which must drop by at least three orders of magnitude, and the class counts
-    must be no worse."""
-    obs, sel, ref = config1_oracle
-    m = compare(run_image(pipe, obs, G.Precision.MIXED), sel, ref)
-    f = compare(run_image(pipe, obs, G.Precision.FP32), sel, ref)
+    """The precision study's acceptance at the same frame policy (rtol 1e-6) on every pixel of the
+    256x256 frame outside the near-critical band, against the binary64 oracle: MIXED's largest
+    error is at or below plain FP32's on every observable, with no slack factor; its event
+    residual, set by binary64 localization, is at least three orders of magnitude smaller."""
+    obs, sel, ref, band = config1_oracle
+    m = compare(run_image(pipe, obs, G.Precision.MIXED), sel[~band], ref[~band])
+    f = compare(run_image(pipe, obs, G.Precision.FP32), sel[~band], ref[~band])
     print("mixed", m, "fp32", f)
     assert m["class_mismatch"] <= f["class_mismatch"]
-    # one tolerance unit: rtol 1e-6 times the observable's scale (angles and relative quantities 1,
-    # hit radius 10 M, travel time 1000 M)
-    unit = dict(escape_direction_rad=1e-6, g_rel=1e-6, hit_radius=1e-5, source_azimuth=1e-6, travel_time=1e-3,
-                max_null_residual=1e-6, max_lz_drift=1e-6, max_carter_drift=1e-6)
-    for k, u in unit.items():
-        assert m[k] <= 1.5 * f[k] + u, (k, m[k], f[k])
+    for k in ("escape_direction_rad", "g_rel", "hit_radius", "source_azimuth", "travel_time", "max_null_residual",
+              "max_lz_drift", "max_carter_drift"):
+        assert m[k] <= f[k], (k, m[k], f[k])
     assert m["event_residual_gpu_max"] <= 1e-3 * f["event_residual_gpu_max"]
