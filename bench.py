@@ -69,11 +69,12 @@ def compact_roofline(r: dict) -> dict:
             "hbm_frac": r["hbm_view"]["frac"]}
 
 
-def make_headline(value, world, steps, warmup, ms_per_step, precision, policy, launches, clk, e2e, roofline) -> dict:
+def make_headline(value, world, steps, warmup, ms_per_step, precision, policy, launches, clk, e2e, roofline,
+                  scaling: str = "weak") -> dict:
     """The last stdout line: the contract keys only, well under 1 KB (the studies go on earlier lines)."""
     return rounded({
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": steps, "warmup": warmup,
-        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": scaling, "vs_baseline": None,
         "dtype": {"fp32": "f32", "mixed": "f32+f64", "fp64": "f64"}[precision],
         "data": "synthetic", "config": compact_config(precision, policy),
         "gpu_launches": int(launches), "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
@@ -313,7 +314,14 @@ def run_gpu(args) -> None:
     dev = torch.device("cuda", local)
     obs = make_observation(G)
     scene = obs.pack()
-    cam = G.image_camera(0, WIDTH, HEIGHT)
+    # weak scaling: every rank traces a frame of its own; strong: the ranks split one frame into
+    # bands of whole tile rows (tile regions on the camera, no collective on the data path)
+    region = None
+    if args.scaling == "strong":
+        from gravlume_b200.shard import region_pixel_rows, shard_region
+
+        region = shard_region(WIDTH, HEIGHT, world, rank)
+    cam = G.image_camera(0, WIDTH, HEIGHT, region=region)
     pipe = G.TracePipeline(local)
     precision = {"fp32": G.Precision.FP32, "mixed": G.Precision.MIXED, "fp64": G.Precision.FP64}[args.precision]
     pipe.set_policy(G.ReferencePolicy.frame(precision, persistent=int(args.persistent)))
@@ -349,8 +357,12 @@ def run_gpu(args) -> None:
 
         total_ms = max_over_ranks(total_ms)
     rays = WIDTH * HEIGHT
-    value = world * rays * args.steps / (total_ms / 1e3) / 1e6
+    frames = world if args.scaling == "weak" else 1
+    value = frames * rays * args.steps / (total_ms / 1e3) / 1e6
     d = results.numpy()
+    if region is not None:  # this rank's band of the frame
+        band = region_pixel_rows(region, WIDTH, HEIGHT)
+        d = {k: v[band.start * WIDTH:band.stop * WIDTH] for k, v in d.items()}
 
     # ---- end to end through the host-buffer call (H2D job table, trace, D2H of every field)
     e2e_ms = None
@@ -369,9 +381,9 @@ def run_gpu(args) -> None:
         from gravlume_b200.shard import max_over_ranks
 
         e2e_ms = max_over_ranks(e2e_ms)  # every rank traces its own frame; the slowest sets the pace
-    e2e = {"value": world * rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+    e2e = {"value": frames * rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
            "h2d_bytes_per_step": int(world * ctypes_sizeof_job()),
-           "d2h_bytes_per_step": int(world * WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
+           "d2h_bytes_per_step": int(frames * WIDTH * HEIGHT * sum(N.RESULT_BYTES.values()))}
 
     if rank != 0:
         if dist:
@@ -384,6 +396,7 @@ def run_gpu(args) -> None:
     attempts = float(d["accepted_steps"].sum() + d["rejected_steps"].sum())
     alg_flops = attempts * flops[2]
     launch_s = (total_ms / args.steps) / 1e3
+    rays_here = rays if region is None else len(band) * WIDTH
     achieved_tflops = alg_flops / launch_s / 1e12
     clk = clocks.summary()
     sm_count = pipe.stats().sm_count
@@ -396,9 +409,9 @@ def run_gpu(args) -> None:
                 "alg_flops_per_launch": alg_flops, "attempted_steps": attempts,
                 "flops_per_attempt": float(flops[2]),
                 "traffic": args.traffic_bytes if args.traffic_bytes is not None else (
-                    TRAFFIC_BYTES_PER_RAY[args.precision] * rays if args.precision in TRAFFIC_BYTES_PER_RAY else None),
+                    TRAFFIC_BYTES_PER_RAY[args.precision] * rays_here if args.precision in TRAFFIC_BYTES_PER_RAY else None),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1280x720, scaled by rays",
-                "algorithmic_bytes_per_launch": float(sum(N.RESULT_BYTES.values())) * rays}
+                "algorithmic_bytes_per_launch": float(sum(N.RESULT_BYTES.values())) * rays_here}
     # the same launch against HBM, to show how far from bandwidth-bound the path is
     hbm_peak, hbm_source = 6650.0, "fallback"
     try:
@@ -410,7 +423,7 @@ def run_gpu(args) -> None:
                             "peak_source": f"{hbm_source} copy bandwidth"}
 
     headline = make_headline(value, world, args.steps, args.warmup, total_ms / args.steps, args.precision, policy,
-                             launches, clk, e2e, roofline)
+                             launches, clk, e2e, roofline, scaling=args.scaling)
     studies = {"roofline_detail": roofline, "class_histogram": np.bincount(d["termination"], minlength=9).tolist(),
                "steps_per_ray": {"mean": float(d["accepted_steps"].mean()), "max": int(d["accepted_steps"].max()),
                                  "rejected_mean": float(d["rejected_steps"].mean())}}
@@ -1120,6 +1133,8 @@ def main() -> None:
                     help="pixels of the frame traced by the CPU oracle (baseline and error report)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch from an ncu capture, reported as roofline.traffic")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="weak: a frame per rank; strong: the ranks split one frame into tile-row bands")
     ap.add_argument("--studies-out", default=None,
                     help="also write the headline and every study to this JSON file")
     ap.add_argument("--width", type=int, default=WIDTH, help="frame width (smaller frames for profiling)")

@@ -39,6 +39,28 @@ def shard_rows(height: int, world: int, rank: int) -> range:
     return range(start, start + base + (1 if rank < extra else 0))
 
 
+def shard_region(width: int, height: int, world: int, rank: int):
+    """The tile region of one frame that `rank` traces: a band of whole 8x8-pixel tile rows (the
+    first ranks take one more row when the rows do not divide evenly), as a TileRegion for
+    glc_camera.tile_origin / tile_count, or None when the rank has no rows. Its results land in the
+    frame's own layout, so the ranks' bands together are the frame."""
+    from .batches import TileRegion, tile_grid
+
+    gx, gy = tile_grid(width, height)
+    rows = shard_rows(gy, world, rank)
+    if len(rows) == 0:
+        return None
+    return TileRegion((0, rows.start), (gx, len(rows)))
+
+
+def region_pixel_rows(region, width: int, height: int) -> range:
+    """Pixel rows a shard_region band covers (clipped to the frame)."""
+    if region is None:
+        return range(0, 0)
+    _, y0, _, y1 = region.pixel_rect(width, height)
+    return range(y0, y1)
+
+
 def max_over_ranks(value: float, group=None) -> float:
     """The largest of the ranks' values (device times are reported as the slowest rank's)."""
     import torch

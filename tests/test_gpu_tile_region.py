@@ -138,3 +138,23 @@ def test_invalid_regions_are_rejected():
         cam = image_camera(0, W, H, region=TileRegion((0, 0), (1, 1)))
         with pytest.raises(G.GlcError):
             pipe.refine_shadow_edges([sc], [cam], one)
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_rank_bands_traced_one_after_another_reassemble_the_frame(world):
+    """The multi-GPU split of one frame (gravlume_b200.shard.shard_region: a band of whole tile rows
+    per rank), each band traced in turn on this GPU into one result set, equals the one-shot frame
+    byte for byte."""
+    from gravlume_b200.shard import shard_region
+
+    obs = config1_observation(width=W, height=H)
+    sc = obs.pack()
+    with G.TracePipeline(0, G.ReferencePolicy.frame(G.Precision.MIXED)) as pipe:
+        one = pipe.trace([sc], [image_camera(0, W, H)])
+        banded = TraceResults(W * H, torch.device("cuda", 0))
+        for rank in range(world):
+            region = shard_region(W, H, world, rank)
+            if region is not None:
+                pipe.trace([sc], [image_camera(0, W, H, region=region)], banded)
+        torch.cuda.synchronize()
+    _assert_equal(_bytes(one), _bytes(banded))

@@ -29,6 +29,19 @@ def test_partitions_cover_every_camera_and_row_once():
     assert max(per) <= sum(counts) / world + max(counts)
 
 
+def test_frame_regions_cover_every_pixel_row_once():
+    from gravlume_b200.shard import region_pixel_rows, shard_region
+
+    for width, height in ((3840, 2160), (1001, 17), (8, 8), (64, 9)):
+        for world in (1, 2, 3, 4, 8):
+            regions = [shard_region(width, height, world, r) for r in range(world)]
+            rows = [i for r in regions for i in region_pixel_rows(r, width, height)]
+            assert rows == list(range(height))
+            for r in regions:
+                if r is not None:
+                    assert r.origin[0] == 0 and r.workgroups[0] == -(-width // 8)
+
+
 def _worker(rank, world, port, height, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
