@@ -201,3 +201,17 @@ def test_policy_presets_follow_the_reference_and_validate():
         assert getattr(s, name) == getattr(O.strict_v1(), name), name
     f = G.ReferencePolicy.frame(G.Precision.FP64)
     assert f.position_rtol == 1e-10 and f.position_atol == 1e-12
+
+
+def test_integration_binding_sizes_match_the_abi():
+    """The Rust binding in INTEGRATION.md declares opaque structs by byte size; those sizes are the
+    C ABI's (as mirrored by the ctypes declarations)."""
+    import ctypes
+    import re
+    from pathlib import Path
+
+    text = (Path(__file__).resolve().parents[1] / "INTEGRATION.md").read_text()
+    sizes = {m.group(1): int(m.group(2)) for m in re.finditer(r"pub struct (glc_\w+) \{ _bytes: \[u8; (\d+)\] \}", text)}
+    assert sizes["glc_policy"] == ctypes.sizeof(N.Policy)
+    assert sizes["glc_scene"] == ctypes.sizeof(N.Scene)
+    assert "pub tile_origin: [u32; 2]" in text and ctypes.sizeof(N.Camera) == 80
