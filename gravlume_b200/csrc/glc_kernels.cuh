@@ -311,7 +311,10 @@ __device__ __forceinline__ void write_result(const glc_results& o, unsigned long
 // integration observables are NaN and the counters zero.
 __device__ __forceinline__ void write_certified(const glc_results& o, unsigned long long slot) {
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
-  const uint32_t code = uint32_t(GLC_TERM_HORIZON) | (1u << 16) | (uint32_t(kFlagCertified) << 20);
+  // like the reference's certified sample (geodesic_acceleration.wgsl:299-311): horizon, with the
+  // horizon event as its candidate
+  const uint32_t code = uint32_t(GLC_TERM_HORIZON) | ((1u << kEvHorizon) << 12) | (1u << 16) |
+                        (uint32_t(kFlagCertified) << 20);
   if (o.code) reinterpret_cast<uint4*>(o.code)[slot] = make_uint4(code, 0u, 0u, 0u);
   if (o.branch) reinterpret_cast<int4*>(o.branch)[slot] = make_int4(0, 0, 0, 0);
   const double2 nn = make_double2(nan, nan);
@@ -332,7 +335,10 @@ __device__ __forceinline__ void write_certified(const glc_results& o, unsigned l
 // nodes (kFlagReconstructed); the other observables are NaN and the counters zero.
 __device__ __forceinline__ void write_reconstructed(const glc_results& o, unsigned long long slot, const double d[3]) {
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
-  const uint32_t code = uint32_t(GLC_TERM_ESCAPE) | (1u << 16) | (uint32_t(kFlagReconstructed) << 20);
+  // like the reference's reconstructed sample (geodesic_acceleration.wgsl:549-560): escape, with the
+  // escape event as its candidate
+  const uint32_t code = uint32_t(GLC_TERM_ESCAPE) | ((1u << kEvEscape) << 12) | (1u << 16) |
+                        (uint32_t(kFlagReconstructed) << 20);
   if (o.code) reinterpret_cast<uint4*>(o.code)[slot] = make_uint4(code, 0u, 0u, 0u);
   if (o.branch) reinterpret_cast<int4*>(o.branch)[slot] = make_int4(0, 0, 0, 0);
   const double2 nn = make_double2(nan, nan);

