@@ -254,9 +254,10 @@ __device__ void adjoint_backward_ray(const JobView& job, const glc_policy& pol, 
       if (pg[k] != 0.0) atomicAdd(g.params + k, pg[k]);
 }
 
-// Grid-stride over the rays: each thread's replay scratch (K attempts of 7 doubles, word-major
-// across the grid's threads) is reused for every ray it takes, so the scratch is bounded by the
-// grid, not by the ray count.
+// A grid of the SMs times the occupancy whose warps take 32 consecutive rays at a time from a
+// counter (counters[5], zeroed before the launch), so that warps with long rays do not hold up the
+// others. Each thread's replay scratch (K attempts of 7 doubles, word-major across the grid's
+// threads) is reused for every ray it takes: the scratch is bounded by the grid, not by the rays.
 template <int P>
 __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K, CkptStore cs,
                                                                const uint4* meta, double* scratch, const double* dl,
@@ -264,8 +265,17 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_
                                                                unsigned int* counters) {
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (unsigned long long gi = tid; gi < job.total; gi += stride)
-    adjoint_backward_ray<P>(job, pol, K, cs, meta, scratch + tid, stride, gi, dl, g, dconst, charge, counters);
+  const unsigned lane = threadIdx.x & 31u;
+  for (;;) {
+    unsigned int base = 0;
+    if (lane == 0) base = atomicAdd(counters + 5, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((unsigned long long)base >= job.total) break;
+    const unsigned long long gi = (unsigned long long)base + lane;
+    if (gi < job.total)
+      adjoint_backward_ray<P>(job, pol, K, cs, meta, scratch + tid, stride, gi, dl, g, dconst, charge, counters);
+    __syncwarp();
+  }
 }
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -565,6 +575,9 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const double* dconst = t->pinhole ? t->d_dconst : nullptr;
+  if (t->n > 0xffffff00ull) return set_error(GLC_ERR_CAPACITY, "the backward pass takes at most 2^32 - 256 rays");
+  const glc_status sm = cuda_status(cudaMemsetAsync(t->d_counters + 5, 0, sizeof(unsigned int), st));
+  if (sm != GLC_OK) return sm;
   if (t->pol.precision == GLC_MIXED)
     adjoint_backward_kernel<kMIXED><<<unsigned(grid), 128, 0, st>>>(t->job(), t->pol, t->K, ckpt_store(t), t->d_meta,
                                                                     t->d_scratch, dl, *out, dconst, t->charge,
