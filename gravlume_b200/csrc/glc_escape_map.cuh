@@ -51,7 +51,9 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) escape_map_no
       RayResult<S> res;
       for (;;) {
         bool use64 = false;
-        if (P == kMIXED) use64 = __any_sync(__activemask(), double(ray.r) < ls.shell_r);
+        // per ray (not per warp): a node's result must not depend on which other nodes share its
+        // warp, so that a frame traced in tile batches equals the frame traced at once
+        if (P == kMIXED) use64 = double(ray.r) < ls.shell_r;
         if (ray_step<P>(ray, ls, pol, res, use64)) break;
       }
       write_result<P>(dst, slot, ray, res, ls);

@@ -370,11 +370,16 @@ __device__ __forceinline__ void write_reconstructed(const glc_results& o, unsign
 #ifndef GLC_MIN_BLOCKS_BULK
 #define GLC_MIN_BLOCKS_BULK 4
 #endif
+#ifndef GLC_MIN_BLOCKS_TAIL
+#define GLC_MIN_BLOCKS_TAIL 2
+#endif
 template <int P>
 struct LaunchShape {
   static constexpr int kMinBlocks =
-      (P == kFP32 || P == kBULK) ? (P == kFP32 ? GLC_MIN_BLOCKS_FP32 : GLC_MIN_BLOCKS_BULK)
-                                 : (P == kMIXED ? GLC_MIN_BLOCKS_MIXED : GLC_MIN_BLOCKS_FP64);
+      P == kFP32 ? GLC_MIN_BLOCKS_FP32
+                 : (P == kBULK ? GLC_MIN_BLOCKS_BULK
+                               : (P == kMIXED ? GLC_MIN_BLOCKS_MIXED
+                                              : (P == kTAIL ? GLC_MIN_BLOCKS_TAIL : GLC_MIN_BLOCKS_FP64)));
 };
 
 template <int P>

@@ -44,6 +44,32 @@ def unit(theta, phi):
     return np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], axis=-1)
 
 
+# A ray is near-critical when the oracle's own answer moves by more than this between rtol 1e-10
+# and rtol 1e-7: its class changes, or its escape direction (rad), hit radius (M) or relative g
+# shifts by more than 1e-5, ten times what the looser tolerance moves a well-conditioned ray. On
+# the 256x256 frame that is 12 of 65,536 rays: higher-order images that cross the equator two or
+# four times before they hit the disk.
+NEAR_CRITICAL_SHIFT = 1e-5
+
+
+def near_critical_band(ref: np.ndarray, loose: np.ndarray) -> np.ndarray:
+    """Rays whose class or observables are decided by less than the frame tolerance's truncation:
+    `ref` and `loose` are the oracle's rows for the same rays at rtol 1e-10 and rtol 1e-7."""
+    t, tl = ref[:, F["termination"]].astype(int), loose[:, F["termination"]].astype(int)
+    band = t != tl
+    esc = ~band & (t == G.Termination.ESCAPE)
+    d0 = np.stack([ref[:, F["escape_dx"]], ref[:, F["escape_dy"]], ref[:, F["escape_dz"]]], axis=1)
+    d1 = np.stack([loose[:, F["escape_dx"]], loose[:, F["escape_dy"]], loose[:, F["escape_dz"]]], axis=1)
+    ang = np.arccos(np.clip(np.nan_to_num((d0 * d1).sum(1), nan=1.0), -1, 1))
+    band |= esc & (ang > NEAR_CRITICAL_SHIFT)
+    ref_g = np.where(ref[:, F["frequency_ratio"]] != 0, ref[:, F["frequency_ratio"]], np.nan)
+    srf = ~band & (t == G.Termination.EQUATORIAL_SURFACE)
+    dr = np.abs(ref[:, F["source_radius"]] - loose[:, F["source_radius"]])
+    dg = np.abs(ref[:, F["frequency_ratio"]] - loose[:, F["frequency_ratio"]]) / np.abs(ref_g)
+    band |= srf & ((np.nan_to_num(dr) > NEAR_CRITICAL_SHIFT) | (np.nan_to_num(dg) > NEAR_CRITICAL_SHIFT))
+    return band
+
+
 def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
     """Per-observable max error of GPU rays `sel` against oracle rows `ref` (matching classes only)."""
     gt = gpu["termination"][sel]

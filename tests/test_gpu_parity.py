@@ -14,7 +14,7 @@ import torch
 
 import gravlume_b200 as G
 import oracle as O
-from gpu_common import F, compare, config1_observation, oracle_for, seeded_pixels
+from gpu_common import F, compare, config1_observation, near_critical_band, oracle_for, seeded_pixels
 
 pytestmark = pytest.mark.gpu
 
@@ -38,8 +38,9 @@ def pipe():
 @pytest.fixture(scope="module")
 def config1_oracle():
     """Every pixel of the 256x256 frame by the oracle at rtol 1e-10 / atol 1e-12, and the
-    near-critical band: the pixels whose oracle class changes when its tolerance is loosened to
-    rtol 1e-7 / atol 1e-9 (their class is decided by less than the frame tolerance's truncation)."""
+    near-critical band: the pixels whose oracle answer moves when its tolerance is loosened to
+    rtol 1e-7 / atol 1e-9 (gpu_common.near_critical_band: decided by less than the frame
+    tolerance's truncation)."""
     obs = config1_observation()
     osc, ev, _ = oracle_for(obs)
     idx = np.arange(256 * 256)
@@ -48,8 +49,8 @@ def config1_oracle():
     ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
     assert (status == 0).all()
     loose, _ = O.trace_pixels(osc, O.custom_policy(1e-7, 1e-9), ev, px, py, threads=threads)
-    band = ref[:, F["termination"]] != loose[:, F["termination"]]
-    assert band.sum() <= 0.005 * idx.size, int(band.sum())
+    band = near_critical_band(ref, loose)
+    assert band.sum() <= 0.01 * idx.size, int(band.sum())
     return obs, idx, ref, band
 
 
@@ -72,12 +73,11 @@ def test_fp64_image_matches_the_oracle_on_every_config1_pixel(pipe, config1_orac
     assert rep["radial_turnings_mismatch"] == 0 and rep["equatorial_crossings_mismatch"] == 0
 
 
-# The same frame policy over every pixel of the frame outside the near-critical band: the rays
-# next to the band (lensed around the photon sphere before they escape or reach the disk) amplify
-# the truncation error, so the largest errors are about twice the sampled ones; 99.9 % of the rays
-# stay within F32_BUDGET.
-F32_EVERY_PIXEL_BUDGET = dict(escape_direction_rad=5e-3, g_rel=1e-2, hit_radius=5e-2, source_azimuth=5e-3,
-                              travel_time=2e-1)
+# The same frame policy over every pixel of the frame outside the near-critical band: the largest
+# errors come from the rays next to the band (lensed around the photon sphere), so the maxima are
+# held to wider budgets and 99.9 % of the rays to F32_BUDGET.
+F32_EVERY_PIXEL_BUDGET = dict(escape_direction_rad=2e-3, g_rel=2e-3, hit_radius=1e-2, source_azimuth=2e-3,
+                              travel_time=5e-2)
 
 
 def per_ray_errors(d, sel, ref):
@@ -127,7 +127,7 @@ def test_full_frame_scene_set_matches_the_oracle(pipe, a, q, incl):
     ref, status = O.trace_pixels(osc, O.custom_policy(1e-10, 1e-12), ev, px, py, threads=threads)
     assert (status == 0).all()
     loose, _ = O.trace_pixels(osc, O.custom_policy(1e-7, 1e-9), ev, px, py, threads=threads)
-    band = ref[:, F["termination"]] != loose[:, F["termination"]]
+    band = near_critical_band(ref, loose)
     sel = (py * w + px)[~band]
     frame_tol = dict(position_rtol=1e-6, momentum_rtol=1e-6, position_atol=1e-8, momentum_atol=1e-8, maximum_step=1e3)
     for precision, extra in ((G.Precision.FP32, {}), (G.Precision.MIXED, {}), (G.Precision.FP64, frame_tol)):
