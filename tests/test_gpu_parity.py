@@ -24,7 +24,7 @@ pytestmark = pytest.mark.gpu
 # integration-tolerance level, not bitwise.
 FP64_BUDGET = dict(escape_direction_rad=1e-7, g_rel=1e-8, hit_radius=1e-7, source_azimuth=1e-7,
                    travel_time=1e-6, max_null_residual=1e-9, max_lz_drift=1e-8, max_carter_drift=1e-8)
-# Binary32 / mixed frame policy (rtol 1e-6, atol 1e-8) against the binary64 oracle.
+# Binary32 / mixed frame policies (FP32 rtol 1e-6, MIXED 7e-7) against the binary64 oracle.
 F32_BUDGET = dict(escape_direction_rad=2e-3, g_rel=1e-3, hit_radius=1e-2, source_azimuth=2e-3, travel_time=5e-2)
 
 
@@ -266,8 +266,8 @@ def test_full_hd_frame_never_exhausts_steps(pipe, precision):
 
 
 def test_mixed_is_at_or_below_plain_fp32_error_on_every_observable(pipe, config1_oracle):
-    """The precision study's acceptance at the same frame policy (rtol 1e-6) on every pixel of the
-    256x256 frame outside the near-critical band, against the binary64 oracle: MIXED's largest
+    """The precision study's acceptance at the frame policies (FP32 rtol 1e-6, MIXED rtol 7e-7) on
+    every pixel of the 256x256 frame outside the near-critical band, against the binary64 oracle: MIXED's largest
     error is at or below plain FP32's on every observable, with no slack factor; its event
     residual, set by binary64 localization, is at least three orders of magnitude smaller."""
     obs, sel, ref, band = config1_oracle
