@@ -101,9 +101,16 @@ __global__ void __launch_bounds__(128) adjoint_forward_kernel(JobView job, glc_p
   }
   const LaneScene ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor);
   Ray<P> ray;
-  ray.init(ls, pol, st8, dir);
   RayResult<S> res;
   uint32_t taken = 0;
+  if (pass == 0) {
+    ray.init(ls, pol, st8, dir);
+  } else {
+    // resume from the last dense checkpoint (the stepper object at accepted step (cap - 1) K):
+    // the same step function from the same object replays pass 0 bit for bit
+    load_ray<P>(ray, cs, cs.cap - 1, base, gi);
+    taken = cs.cap - 1;
+  }
   for (;;) {
     if (ray.accepted == taken * K) {
       if (pass == 0 ? taken < cs.cap : taken >= cs.cap) store_ray<P>(ray, cs, taken, base, gi);
