@@ -284,63 +284,12 @@ bool split_mixed(const glc_policy& pol) {
 
 size_t handoff_bytes(unsigned long long rays) { return size_t(rays) * kHandoffWords * sizeof(uint4); }
 
-constexpr unsigned long long kSplitBandRays = 1ull << 20;
-constexpr int kMaxSplitBands = 16;
-
-glc_status ensure_split_streams(glc_ctx* ctx) {
-  int least = 0, greatest = 0;
-  GLC_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-  if (!ctx->split_stream[0]) GLC_CUDA(cudaStreamCreateWithPriority(&ctx->split_stream[0], cudaStreamNonBlocking, least));
-  if (!ctx->split_stream[1])
-    GLC_CUDA(cudaStreamCreateWithPriority(&ctx->split_stream[1], cudaStreamNonBlocking, greatest));
-  if (!ctx->split_entry) GLC_CUDA(cudaEventCreateWithFlags(&ctx->split_entry, cudaEventDisableTiming));
-  if (!ctx->split_done) GLC_CUDA(cudaEventCreateWithFlags(&ctx->split_done, cudaEventDisableTiming));
-  for (cudaEvent_t& e : ctx->split_band)
-    if (!e) GLC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  return GLC_OK;
-}
-
 glc_status launch_split(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out,
                         cudaStream_t stream, unsigned char* handoff) {
   const unsigned block = pol.block_threads;
   const unsigned long long grid = (job.total + block - 1) / block;
   if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
   const Handoff hv{reinterpret_cast<uint4*>(handoff), job.total};
-  const unsigned long long nb =
-      std::min<unsigned long long>(kMaxSplitBands, std::max<unsigned long long>(1, job.total / kSplitBandRays));
-  if (nb > 1) {
-    // bands of whole blocks: the bulk kernels of all bands in order on one stream, each band's
-    // completion on the second stream as soon as its bulk kernel is done
-    glc_status s = ensure_split_streams(ctx);
-    if (s != GLC_OK) return s;
-    cudaStream_t sb = ctx->split_stream[0], st = ctx->split_stream[1];
-    GLC_CUDA(cudaEventRecord(ctx->split_entry, stream));
-    GLC_CUDA(cudaStreamWaitEvent(sb, ctx->split_entry, 0));
-    GLC_CUDA(cudaStreamWaitEvent(st, ctx->split_entry, 0));
-    const unsigned long long per = ((grid + nb - 1) / nb) * block;
-    int k = 0;
-    for (unsigned long long g0 = 0; g0 < job.total; g0 += per, ++k) {
-      JobView jb = job;
-      jb.total = std::min(g0 + per, job.total);
-      const unsigned bg = unsigned((jb.total - g0 + block - 1) / block);
-      trace_bulk_kernel<kBULK><<<bg, block, 0, sb>>>(jb, pol, out, hv, g0);
-      GLC_CUDA(cudaGetLastError());
-      GLC_CUDA(cudaEventRecord(ctx->split_band[k], sb));
-      GLC_CUDA(cudaStreamWaitEvent(st, ctx->split_band[k], 0));
-      trace_tail_kernel<kTAIL><<<bg, block, 0, st>>>(jb, pol, out, hv, g0);
-      GLC_CUDA(cudaGetLastError());
-      ctx->stats.kernel_launches += 2;
-    }
-    // join both streams back into the caller's (a graph capture needs every forked stream joined)
-    GLC_CUDA(cudaEventRecord(ctx->split_done, st));
-    GLC_CUDA(cudaStreamWaitEvent(stream, ctx->split_done, 0));
-    GLC_CUDA(cudaStreamWaitEvent(stream, ctx->split_band[k - 1], 0));
-    ctx->stats.last_grid = unsigned(grid);
-    ctx->stats.last_block = block;
-    ctx->stats.last_persistent = 0;
-    ctx->stats.last_rays = job.total;
-    return GLC_OK;
-  }
   trace_bulk_kernel<kBULK><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
   GLC_CUDA(cudaGetLastError());
   trace_tail_kernel<kTAIL><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
@@ -724,12 +673,6 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_footprint) cudaFree(ctx->d_footprint);
   if (ctx->d_host_ws) cudaFree(ctx->d_host_ws);
   if (ctx->d_handoff) cudaFree(ctx->d_handoff);
-  for (cudaStream_t c : ctx->split_stream)
-    if (c) cudaStreamDestroy(c);
-  for (cudaEvent_t e : ctx->split_band)
-    if (e) cudaEventDestroy(e);
-  if (ctx->split_entry) cudaEventDestroy(ctx->split_entry);
-  if (ctx->split_done) cudaEventDestroy(ctx->split_done);
   for (cudaEvent_t e : ctx->host_band)
     if (e) cudaEventDestroy(e);
   if (ctx->host_entry) cudaEventDestroy(ctx->host_entry);

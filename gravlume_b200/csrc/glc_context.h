@@ -30,12 +30,6 @@ struct glc_ctx {
   unsigned char* d_host_ws = nullptr;  // device workspace of glc_trace_host (grow-only)
   unsigned char* d_handoff = nullptr;  // MIXED two-kernel hand-off records (grow-only)
   size_t d_handoff_bytes = 0;
-  // MIXED two-kernel pipeline: bands of the job run the bulk kernel on one stream and, band by
-  // band, the completion kernel on a second (higher-priority) stream, so that the binary64
-  // completion of one band overlaps the binary32 stepping of the next
-  cudaStream_t split_stream[2] = {};
-  cudaEvent_t split_entry = nullptr, split_done = nullptr;
-  cudaEvent_t split_band[16] = {};
   cudaStream_t host_compute[2] = {};  // glc_trace_host: bands are traced on two streams in turn ...
   cudaStream_t host_copy = nullptr;    // ... and copied back on a third
   cudaEvent_t host_upload = nullptr;   // the job table is on the device
