@@ -241,7 +241,7 @@ namespace {
 
 template <int P>
 glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out,
-                            cudaStream_t stream, unsigned long long* queue) {
+                            cudaStream_t stream, unsigned long long* queue, Handoff hv = Handoff{nullptr, 0}) {
   const unsigned block = pol.block_threads;
   if (pol.persistent) {
     int per_sm = int(pol.blocks_per_sm);
@@ -258,9 +258,9 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
     if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
     GLC_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream));
     if (pol.persistent == 2)
-      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue, hv);
     else
-      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue, hv);
     ctx->stats.last_grid = unsigned(grid);
     ctx->stats.kernel_launches += 1;
   } else {
@@ -277,27 +277,32 @@ glc_status launch_precision(glc_ctx* ctx, const JobView& job, const glc_policy& 
   return GLC_OK;
 }
 
-// MIXED as two kernels (binary32 bulk, then binary64 completion) over the hand-off records.
-bool split_mixed(const glc_policy& pol) {
-  return pol.precision == GLC_MIXED && pol.persistent == 0 && pol.mixed_split != 0;
-}
+// MIXED as two kernels (binary32 bulk, then binary64 completion) over the hand-off records; the
+// bulk kernel is the one-thread-per-ray kernel or, with `persistent`, a work-queue kernel.
+bool split_mixed(const glc_policy& pol) { return pol.precision == GLC_MIXED && pol.mixed_split != 0; }
 
 size_t handoff_bytes(unsigned long long rays) { return size_t(rays) * kHandoffWords * sizeof(uint4); }
 
 glc_status launch_split(glc_ctx* ctx, const JobView& job, const glc_policy& pol, const glc_results& out,
-                        cudaStream_t stream, unsigned char* handoff) {
+                        cudaStream_t stream, unsigned char* handoff, unsigned long long* queue) {
   const unsigned block = pol.block_threads;
   const unsigned long long grid = (job.total + block - 1) / block;
   if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
   const Handoff hv{reinterpret_cast<uint4*>(handoff), job.total};
-  trace_bulk_kernel<kBULK><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
-  GLC_CUDA(cudaGetLastError());
+  if (pol.persistent) {
+    const glc_status s = launch_precision<kBULK>(ctx, job, pol, out, stream, queue, hv);
+    if (s != GLC_OK) return s;
+  } else {
+    trace_bulk_kernel<kBULK><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
+    GLC_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+  }
   trace_tail_kernel<kTAIL><<<unsigned(grid), block, 0, stream>>>(job, pol, out, hv, 0ull);
   GLC_CUDA(cudaGetLastError());
-  ctx->stats.last_grid = unsigned(grid);
-  ctx->stats.kernel_launches += 2;
+  if (!pol.persistent) ctx->stats.last_grid = unsigned(grid);
+  ctx->stats.kernel_launches += 1;
   ctx->stats.last_block = block;
-  ctx->stats.last_persistent = 0;
+  ctx->stats.last_persistent = pol.persistent;
   ctx->stats.last_rays = job.total;
   return GLC_OK;
 }
@@ -340,7 +345,7 @@ glc_status launch(glc_ctx* ctx, const JobView& job_in, const glc_policy& pol, co
     ctx->stats.kernel_launches += 1;
     job.emap = emap;
   }
-  if (split_mixed(pol) && handoff) return launch_split(ctx, job, pol, out, stream, handoff);
+  if (split_mixed(pol) && handoff) return launch_split(ctx, job, pol, out, stream, handoff, queue);
   switch (pol.precision) {
     case GLC_FP32: return launch_precision<kFP32>(ctx, job, pol, out, stream, queue);
     case GLC_MIXED: return launch_precision<kMIXED>(ctx, job, pol, out, stream, queue);

@@ -452,16 +452,14 @@ __device__ __forceinline__ uint32_t handoff_resume(const Handoff& hv, unsigned l
   return handoff_unpack(rec, ray, sc, st8, direction, failure);
 }
 
-// MIXED, first kernel: one thread per ray, binary32 stepping with the compensated pair state at
-// the binary32 register budget. Non-terminal turning points and equatorial crossings are handled
-// here; a ray leaves at the start of its first step that brackets a terminal event (or a surface
-// crossing near the surface), or when it enters the binary64 shell, or when it fails, by storing
-// its hand-off record. Certified and map-reconstructed pixels are written here.
-template <int P = kBULK>
-__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
-    trace_bulk_kernel(JobView job, glc_policy pol, glc_results out, Handoff hv, unsigned long long base) {
-  static_assert(P == kBULK, "the bulk kernel steps the BULK precision");
-  const unsigned long long gi = base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+// MIXED, first kernel: binary32 stepping with the compensated pair state at the binary32 register
+// budget. Non-terminal turning points and equatorial crossings are handled here; a ray leaves at the
+// start of its first step that brackets a terminal event (or a surface crossing near the surface),
+// or when it enters the binary64 shell, or when it fails, by storing its hand-off record.
+// Certified and map-reconstructed pixels are written here. bulk_one is one ray of it, shared by
+// the one-thread-per-ray kernel and the work-queue kernels.
+__device__ __forceinline__ void bulk_one(const JobView& job, const glc_policy& pol, const glc_results& out,
+                                         const Handoff& hv, unsigned long long gi) {
   if (gi >= job.total) return;
   double st8[8], dir;
   unsigned long long slot;
@@ -480,6 +478,13 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
   while (!ray.step(ls, pol, res, false)) {
   }
   handoff_store(hv, gi, ray, res);
+}
+
+template <int P = kBULK>
+__global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
+    trace_bulk_kernel(JobView job, glc_policy pol, glc_results out, Handoff hv, unsigned long long base) {
+  static_assert(P == kBULK, "the bulk kernel steps the BULK precision");
+  bulk_one(job, pol, out, hv, base + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // MIXED, second kernel: one thread per ray of the same job; resumes each handed-off ray in binary64
@@ -518,7 +523,8 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
 template <int P>
 __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_queue_kernel(JobView job, glc_policy pol,
                                                                                       glc_results out,
-                                                                                      unsigned long long* queue) {
+                                                                                      unsigned long long* queue,
+                                                                                      Handoff hv) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned grab = pol.rays_per_grab < 32u ? 32u : (pol.rays_per_grab & ~31u);
@@ -527,7 +533,10 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_queue_k
     if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
     base = __shfl_sync(FULL, base, 0);
     if (base >= job.total) break;
-    for (unsigned k = 0; k < grab; k += 32u) trace_one<P>(job, pol, out, base + k + lane);
+    for (unsigned k = 0; k < grab; k += 32u) {
+      if constexpr (P == kBULK) bulk_one(job, pol, out, hv, base + k + lane);
+      else trace_one<P>(job, pol, out, base + k + lane);
+    }
   }
 }
 
@@ -539,7 +548,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_queue_k
 // has no waits on other warps or blocks.
 template <int P>
 __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persistent_kernel(JobView job, glc_policy pol, glc_results out,
-                                                               unsigned long long* queue) {
+                                                               unsigned long long* queue, Handoff hv) {
   using S = typename PrecTraits<P>::S;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -547,7 +556,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
   Ray<P> ray;
   RayResult<S> res;
   LaneScene ls;
-  unsigned long long slot = 0;
+  unsigned long long slot = 0, ray_index = 0;
   bool active = false;
   unsigned long long grab_next = 0, grab_end = 0;
   bool drained = false;
@@ -586,6 +595,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
             } else {
               ls = make_lane_scene(job.scenes[scene_idx], pol.mixed_shell_factor, out.drift_a || out.drift_b || pol.uncertain_terminals);
               ray.init(ls, pol, st8, dir);
+              ray_index = grab_next + rank;
               active = true;
             }
           }
@@ -603,7 +613,8 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_persist
     if (P == kMIXED) use64 = __any_sync(FULL, active && double(ray.r) < ls.shell_r);
     if (active) {
       if (ray_step<P>(ray, ls, pol, res, use64)) {
-        write_result<P>(out, slot, ray, res, ls);
+        if constexpr (P == kBULK) handoff_store(hv, ray_index, ray, res);
+        else write_result<P>(out, slot, ray, res, ls);
         active = false;
       }
     }

@@ -94,9 +94,9 @@ glc_status launch_static(int device, const JobView& job, const glc_policy& pol, 
     const unsigned long long grid_cap = (warps_needed * 32 + block - 1) / block;
     if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
     if (pol.persistent == 2)
-      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+      trace_queue_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue, Handoff{nullptr, 0});
     else
-      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue);
+      trace_persistent_kernel<P><<<unsigned(grid), block, 0, stream>>>(job, pol, out, queue, Handoff{nullptr, 0});
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(GLC_ERR_CUDA, cudaGetErrorString(e));

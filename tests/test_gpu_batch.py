@@ -140,3 +140,18 @@ def test_batch_sample_matches_the_oracle(pipe, job):
         assert rep["class_mismatch"] == 0, (i, rep)
         if "travel_time" in rep:
             assert rep["travel_time"] <= 1e-6 * max(1.0, m["observer_radius"]), (i, rep)
+
+
+@pytest.mark.parametrize("persistent", [1, 2])
+def test_mixed_work_queue_kernels_run_the_two_kernel_form(pipe, job, persistent):
+    """MIXED through the lane-refill and the warp-grab work queues: the binary32 bulk stepping runs
+    in the queue kernel and the binary64 completion after it, and every ray ends as it does in the
+    one-thread-per-ray launch (the same per-ray code in differently inlined kernels)."""
+    scenes, cams, slots, _ = job
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED, persistent=0))
+    simple = trace(pipe, scenes, cams, slots)
+    pipe.set_policy(G.ReferencePolicy.frame(G.Precision.MIXED, persistent=persistent))
+    queued = trace(pipe, scenes, cams, slots)
+    assert pipe.stats().last_persistent == persistent
+    assert np.all(queued["f64_steps"][queued["flags"] & 0x30 == 0] >= 1), "every integrated ray was completed"
+    assert_same(queued, simple, slice(None))

@@ -87,7 +87,10 @@ def test_static_scratch_trace_matches_glc_trace_on_two_calls_in_a_row():
         (config1_observation(width=160, height=96), 64,
          G.ReferencePolicy.frame(G.Precision.FP64, persistent=1)),
         (config1_observation(width=128, height=128, incl_deg=60.0), 0,
-         G.ReferencePolicy.frame(G.Precision.MIXED, persistent=1, rays_per_grab=32, refill_interval=2)),
+         # the no-allocation entry runs MIXED as one kernel (it has no room for hand-off records),
+         # so the context path is asked for the same form
+         G.ReferencePolicy.frame(G.Precision.MIXED, persistent=1, rays_per_grab=32, refill_interval=2,
+                                 mixed_split=0)),
     ]
     for obs, n_list, policy in jobs:
         scenes, cams, keep, slots = _job(obs, n_list)
