@@ -163,7 +163,7 @@ __device__ void adjoint_backward_ray(const JobView& job, const glc_policy& pol, 
   }
   double lam[6] = {0, 0, 0, 0, 0, 0}, gacc[3] = {0, 0, 0};
   const bool differentiable = status == 1u && (m.y == GLC_TERM_SURFACE || m.y == GLC_TERM_ESCAPE);
-  bool ok = differentiable && any;
+  bool ok = differentiable && any && scratch != nullptr;
   bool degenerate = false;
   double wst[7];
   step_weights(wst);
@@ -261,27 +261,41 @@ __device__ void adjoint_backward_ray(const JobView& job, const glc_policy& pol, 
       if (pg[k] != 0.0) atomicAdd(g.params + k, pg[k]);
 }
 
-// A grid of the SMs times the occupancy whose warps take 32 consecutive rays at a time from a
-// counter (counters[5], zeroed before the launch), so that warps with long rays do not hold up the
-// others. Each thread's replay scratch (K attempts of 7 doubles, word-major across the grid's
-// threads) is reused for every ray it takes: the scratch is bounded by the grid, not by the rays.
+// One thread per ray. The replay scratch (K attempts of 7 doubles per thread) is not per ray: a
+// block borrows one of n_slots scratch slots (busy flags, one per slot) for its lifetime, and
+// there are more slots than blocks that can be resident at once, so the scratch is bounded by the
+// GPU's residency, not by the ray count. Taking a slot is a bounded search over the flags, which
+// always finds a free one while n_slots exceeds the resident blocks; should it ever not, the
+// block's rays get zero gradients and counters[6] records it.
 template <int P>
 __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K, CkptStore cs,
-                                                               const uint4* meta, double* scratch, const double* dl,
-                                                               glc_grads g, const double* dconst, double charge,
+                                                               const uint4* meta, double* scratch, unsigned int* busy,
+                                                               unsigned int n_slots, const double* dl, glc_grads g,
+                                                               const double* dconst, double charge,
                                                                unsigned int* counters) {
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned lane = threadIdx.x & 31u;
-  for (;;) {
-    unsigned int base = 0;
-    if (lane == 0) base = atomicAdd(counters + 5, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if ((unsigned long long)base >= job.total) break;
-    const unsigned long long gi = (unsigned long long)base + lane;
-    if (gi < job.total)
-      adjoint_backward_ray<P>(job, pol, K, cs, meta, scratch + tid, stride, gi, dl, g, dconst, charge, counters);
-    __syncwarp();
+  __shared__ unsigned int slot_s;
+  if (threadIdx.x == 0) {
+    unsigned int s = blockIdx.x % n_slots, found = n_slots;
+    for (unsigned int it = 0; it < 4u * n_slots; ++it) {
+      if (atomicCAS(busy + s, 0u, 1u) == 0u) {
+        found = s;
+        break;
+      }
+      s = s + 1u == n_slots ? 0u : s + 1u;
+    }
+    if (found == n_slots) atomicAdd(counters + 6, 1u);
+    slot_s = found;
+  }
+  __syncthreads();
+  const unsigned int slot = slot_s;
+  const unsigned long long stride = (unsigned long long)n_slots * blockDim.x;
+  double* mine = slot < n_slots ? scratch + (unsigned long long)slot * blockDim.x + threadIdx.x : nullptr;
+  const unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi < job.total) adjoint_backward_ray<P>(job, pol, K, cs, meta, mine, stride, gi, dl, g, dconst, charge, counters);
+  __syncthreads();
+  if (threadIdx.x == 0 && slot < n_slots) {
+    __threadfence();
+    atomicExch(busy + slot, 0u);
   }
 }
 
@@ -327,6 +341,8 @@ struct glc_tape {
   double* d_scratch = nullptr;
   size_t scratch_bytes = 0;
   unsigned int* d_counters = nullptr;
+  unsigned int* d_busy = nullptr;       // backward scratch slots in use (one flag per slot)
+  unsigned int busy_slots = 0;
   bool pinhole = false;
   bool valid = false;  // the last forward pass into the tape completed (backward needs it)
 
@@ -356,6 +372,7 @@ void free_tape(glc_tape* t) {
   if (t->d_dconst) cudaFree(t->d_dconst);
   if (t->d_scratch) cudaFree(t->d_scratch);
   if (t->d_counters) cudaFree(t->d_counters);
+  if (t->d_busy) cudaFree(t->d_busy);
   delete t;
 }
 
@@ -562,16 +579,15 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
   if (!t || !dl || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
   if (!t->valid) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape's last forward pass failed; run it again");
   DeviceScope scope(t->ctx->device);
-  // a grid of the SMs times the kernel's occupancy; each thread keeps K attempts of 7 doubles
+  // scratch slots: twice the blocks that can be resident at once (the SMs times the kernel's
+  // occupancy), each slot K attempts of 7 doubles for each of the block's 128 threads
   int per_sm = 0;
   glc_status s0 = cuda_status(t->pol.precision == GLC_MIXED
                                   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kMIXED>, 128, 0)
                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kFP64>, 128, 0));
   if (s0 != GLC_OK) return s0;
-  unsigned long long grid = (unsigned long long)t->ctx->sm_count * (per_sm > 0 ? per_sm : 1);
-  const unsigned long long grid_cap = (t->n + 127) / 128;
-  if (grid > grid_cap) grid = grid_cap < 1 ? 1 : grid_cap;
-  const size_t need = size_t(t->K) * 7 * sizeof(double) * grid * 128;
+  const unsigned int n_slots = unsigned(2 * t->ctx->sm_count * (per_sm > 0 ? per_sm : 1));
+  const size_t need = size_t(t->K) * 7 * sizeof(double) * n_slots * 128;
   if (need > t->scratch_bytes) {
     if (t->d_scratch) cudaFree(t->d_scratch);
     t->d_scratch = nullptr;
@@ -580,19 +596,28 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
       return set_error(GLC_ERR_CUDA, "adjoint scratch allocation failed");
     t->scratch_bytes = need;
   }
+  if (n_slots > t->busy_slots) {
+    if (t->d_busy) cudaFree(t->d_busy);
+    t->d_busy = nullptr;
+    t->busy_slots = 0;
+    if (cudaMalloc(&t->d_busy, n_slots * sizeof(unsigned int)) != cudaSuccess)
+      return set_error(GLC_ERR_CUDA, "adjoint scratch allocation failed");
+    t->busy_slots = n_slots;
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const double* dconst = t->pinhole ? t->d_dconst : nullptr;
-  if (t->n > 0xffffff00ull) return set_error(GLC_ERR_CAPACITY, "the backward pass takes at most 2^32 - 256 rays");
-  const glc_status sm = cuda_status(cudaMemsetAsync(t->d_counters + 5, 0, sizeof(unsigned int), st));
+  const unsigned long long grid = (t->n + 127) / 128;
+  if (grid > 0x7fffffffull) return set_error(GLC_ERR_CAPACITY, "too many rays for one launch");
+  const glc_status sm = cuda_status(cudaMemsetAsync(t->d_busy, 0, n_slots * sizeof(unsigned int), st));
   if (sm != GLC_OK) return sm;
   if (t->pol.precision == GLC_MIXED)
     adjoint_backward_kernel<kMIXED><<<unsigned(grid), 128, 0, st>>>(t->job(), t->pol, t->K, ckpt_store(t), t->d_meta,
-                                                                    t->d_scratch, dl, *out, dconst, t->charge,
-                                                                    t->d_counters);
+                                                                    t->d_scratch, t->d_busy, n_slots, dl, *out, dconst,
+                                                                    t->charge, t->d_counters);
   else
     adjoint_backward_kernel<kFP64><<<unsigned(grid), 128, 0, st>>>(t->job(), t->pol, t->K, ckpt_store(t), t->d_meta,
-                                                                   t->d_scratch, dl, *out, dconst, t->charge,
-                                                                   t->d_counters);
+                                                                   t->d_scratch, t->d_busy, n_slots, dl, *out, dconst,
+                                                                   t->charge, t->d_counters);
   const glc_status s = cuda_status(cudaGetLastError());
   if (s == GLC_OK) t->ctx->stats.kernel_launches += 1;
   return s;
