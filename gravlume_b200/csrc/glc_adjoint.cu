@@ -263,10 +263,11 @@ __device__ void adjoint_backward_ray(const JobView& job, const glc_policy& pol, 
 
 // One thread per ray. The replay scratch (K attempts of 7 doubles per thread) is not per ray: a
 // block borrows one of n_slots scratch slots (busy flags, one per slot) for its lifetime, and
-// there are more slots than blocks that can be resident at once, so the scratch is bounded by the
-// GPU's residency, not by the ray count. Taking a slot is a bounded search over the flags, which
-// always finds a free one while n_slots exceeds the resident blocks; should it ever not, the
-// block's rays get zero gradients and counters[6] records it.
+// there are as many slots as blocks that can be resident at once, so the scratch is bounded by the
+// GPU's residency, not by the ray count. A block starts only once another has left, and a block
+// frees its slot before it leaves, so a starting block always finds a free slot; the search is
+// bounded (four rounds over the flags, long enough for a release still in flight to land), and
+// should it ever fail, the block's rays get zero gradients and counters[6] records it.
 template <int P>
 __global__ void __launch_bounds__(128) adjoint_backward_kernel(JobView job, glc_policy pol, uint32_t K, CkptStore cs,
                                                                const uint4* meta, double* scratch, unsigned int* busy,
@@ -579,14 +580,14 @@ glc_status glc_backward(glc_tape* t, const double* dl, const glc_grads* out, voi
   if (!t || !dl || !out) return set_error(GLC_ERR_INVALID_ARGUMENT, "null pointer");
   if (!t->valid) return set_error(GLC_ERR_INVALID_ARGUMENT, "the tape's last forward pass failed; run it again");
   DeviceScope scope(t->ctx->device);
-  // scratch slots: twice the blocks that can be resident at once (the SMs times the kernel's
+  // scratch slots: one per block that can be resident at once (the SMs times the kernel's
   // occupancy), each slot K attempts of 7 doubles for each of the block's 128 threads
   int per_sm = 0;
   glc_status s0 = cuda_status(t->pol.precision == GLC_MIXED
                                   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kMIXED>, 128, 0)
                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_backward_kernel<kFP64>, 128, 0));
   if (s0 != GLC_OK) return s0;
-  const unsigned int n_slots = unsigned(2 * t->ctx->sm_count * (per_sm > 0 ? per_sm : 1));
+  const unsigned int n_slots = unsigned(t->ctx->sm_count * (per_sm > 0 ? per_sm : 1));
   const size_t need = size_t(t->K) * 7 * sizeof(double) * n_slots * 128;
   if (need > t->scratch_bytes) {
     if (t->d_scratch) cudaFree(t->d_scratch);

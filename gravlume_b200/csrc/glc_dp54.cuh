@@ -283,10 +283,14 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
     } else {
       kn_rhs<C, false>(k, ys, E, d, rr, vv);
     }
+    // pending sums of the stages still ahead (stage j + 2 + m <= 7); the rest would only add
+    // zero coefficients
 #pragma unroll
-    for (int m = 0; m < 5; ++m)
+    for (int m = 0; m < 5; ++m) {
+      if (m + j > 5) break;
 #pragma unroll
       for (int c = 0; c < 6; ++c) P[m][c] = P[m + 1][c] + Coef::a(j, m) * d[c];
+    }
     const C ej = Coef::e(j);
 #pragma unroll
     for (int c = 0; c < 7; ++c) err[c] += ej * d[c];

@@ -172,6 +172,7 @@ struct Invariants {
 template <class T, bool kInv = false>
 GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_out, Invariants<T>* inv = nullptr) {
   const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
+  // the radius exactly as kn_radius_squared forms it, so both give the same r
   const T R2 = x * x + yy * yy + z * z;
   const T b = R2 - k.a2;
   const T az2 = k.a2 * z * z;
@@ -186,44 +187,48 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
   const T r = r2 * inv_r;
   const T inv_r2 = inv_r * inv_r;
   const T A = r2 + k.a2;
-  const T sigma = r2 + az2 * inv_r2;  // (r^4 + a^2 z^2) / r^2
+  const T m = az2 * inv_r2;  // a^2 z^2 / r^2
+  const T sigma = r2 + m;    // (r^4 + a^2 z^2) / r^2
   // one reciprocal for both denominators: 1/A = sigma/(A sigma), 1/sigma = A/(A sigma)
   const T inv_As = g_rcp(A * sigma);
   const T inv_A = sigma * inv_As;
   const T inv_sigma = A * inv_As;
+  // The chart sign s = +-1 factors out of the null vector l = s lt, of e = s et and of C = s Ct
+  // (s^2 = 1 turns s a into sa inside them), so it enters once, through q and fqs = f q s.
+  // lt = ((r x + sa y) / A, (r y - sa x) / A, z / r)
+  const T lzt = z * inv_r;
+  const T lxt = (r * x + k.sa * yy) * inv_A;
+  const T lyt = (r * yy - k.sa * x) * inv_A;
   // grad r = (x r, y r, z A / r) / sigma
   const T rs = r * inv_sigma;
-  const T grx = x * rs, gry = yy * rs, grz = z * A * inv_r * inv_sigma;
-  // f = (2 r - Q^2) / sigma ; grad f = (2 grad r - f grad sigma) / sigma,
-  // grad sigma = 2 (r - a^2 z^2 / r^3) grad r + (0, 0, 2 a^2 z / r^2)
+  const T grx = x * rs, gry = yy * rs, grz = lzt * (A * inv_sigma);
+  // f = (2 r - Q^2) / sigma; grad f = c1 grad r - (0, 0, 2 a^2 z f / (r^2 sigma)) with
+  // c1 = (2 - 2 f (r - a^2 z^2 / r^3)) / sigma, carried as c1h = c1 / 2
   const T f = (T(2) * r - k.q2) * inv_sigma;
-  const T srf = T(2) * (r - az2 * inv_r2 * inv_r);
-  const T c1 = (T(2) - f * srf) * inv_sigma;
-  const T gfx = c1 * grx, gfy = c1 * gry;
-  const T gfz = c1 * grz - f * (T(2) * k.a2 * z * inv_r2) * inv_sigma;
-  // null vector l
-  const T lx = k.s * (r * x + k.sa * yy) * inv_A;
-  const T ly = k.s * (r * yy - k.sa * x) * inv_A;
-  const T lz = k.s * z * inv_r;
-  const T q = E + lx * px + ly * py + lz * pz;
+  const T c1h = (T(1) - f * (r - m * inv_r)) * inv_sigma;
+  // q = E + l . p
+  const T lxy = lxt * px + lyt * py;
+  const T lzp = lzt * pz;
+  const T q = E + k.s * (lxy + lzp);
   const T fq = f * q;
-  const T vx = px - fq * lx, vy = py - fq * ly, vz = pz - fq * lz;
-  // w = e + C grad r
-  const T sr = k.s * r;
-  const T ex = (sr * px - k.a * py) * inv_A;
-  const T ey = (k.a * px + sr * py) * inv_A;
-  const T ez = k.s * pz * inv_r;
-  const T C = ((k.s * x - T(2) * r * lx) * px + (k.s * yy - T(2) * r * ly) * py) * inv_A - k.s * z * pz * inv_r2;
-  const T hq2 = T(0.5) * q * q;
-  d[0] = vx;
-  d[1] = vy;
-  d[2] = vz;
-  d[3] = fq * (ex + C * grx) + hq2 * gfx;
-  d[4] = fq * (ey + C * gry) + hq2 * gfy;
-  d[5] = fq * (ez + C * grz) + hq2 * gfz;
+  const T fqs = k.s * fq;
+  // Ct = ((x - 2 r lt_x) p_x + (y - 2 r lt_y) p_y) / A - z p_z / r^2
+  const T Ct = (x * px + yy * py - (r + r) * lxy) * inv_A - lzp * inv_r;
+  // p' = f q (e + C grad r) + q^2 / 2 grad f = fqs et + K grad r - q^2 (0, 0, a^2 z f / (r^2 sigma))
+  // with et = ((r p_x - sa p_y) / A, (sa p_x + r p_y) / A, p_z / r) and K = fqs Ct + q^2 c1h
+  const T qq = q * q;
+  const T K = fqs * Ct + qq * c1h;
+  const T W = fqs * inv_A;
+  const T gz = f * inv_sigma * lzt * inv_r * k.a2;
+  d[0] = px - fqs * lxt;
+  d[1] = py - fqs * lyt;
+  d[2] = pz - fqs * lzt;
+  d[3] = W * (r * px - k.sa * py) + K * grx;
+  d[4] = W * (k.sa * px + r * py) + K * gry;
+  d[5] = (fqs * inv_r) * pz + K * grz - qq * gz;
   d[6] = E + fq;
   r_out = r;
-  vr_out = grx * vx + gry * vy + grz * vz;
+  vr_out = grx * d[0] + gry * d[1] + grz * d[2];
   if (kInv && inv != nullptr) {
     // Carter's constant as Q = L_x^2 + L_y^2 + a^2 [(z^2/r^2)(P_perp^2 - E^2) - (rho^2/A) p_z^2]
     // (see kn_invariants): no r^2-sized terms cancel, so binary32 keeps its relative accuracy far out
@@ -234,9 +239,9 @@ GLC_HD void kn_rhs(const KN<T>& k, const T y[6], T E, T d[7], T& r_out, T& vr_ou
     inv->abracket = k.a2 * (z * z * inv_r2 * (pp2 - E * E) - rho2 * inv_A * pz * pz);
     inv->carter = Lx * Lx + Ly * Ly + inv->abracket;
     // g^{mu nu} p_mu p_nu with m = eta - f l l and u_i = l^i p_i (u_0 = E): diagonal terms
-    // eta_ii p_i^2 - f u_i^2, off-diagonal -f u_i u_j
-    const T u1 = lx * px, u2 = ly * py, u3 = lz * pz;
-    const T sum = -E * E + pp2 + pz * pz - f * q * q;
+    // eta_ii p_i^2 - f u_i^2, off-diagonal -f u_i u_j (only u_i^2 and |u_i| enter, so lt serves)
+    const T u1 = lxt * px, u2 = lyt * py, u3 = lzp;
+    const T sum = -E * E + pp2 + pz * pz - f * qq;
     const T au = g_abs(E) + g_abs(u1) + g_abs(u2) + g_abs(u3);
     const T su2 = E * E + u1 * u1 + u2 * u2 + u3 * u3;
     const T norm = E * E * g_abs(T(1) + f) + g_abs(px * px - f * u1 * u1) + g_abs(py * py - f * u2 * u2) +

@@ -612,7 +612,6 @@ struct Ray {
       o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
                                      finite);
 #endif
-      if (pair && sc.track) pair_invariants_after(o);
     }
     if (!finite || !g_finite(o.en)) {
       finish_plain(res, GLC_TERM_NUMERICAL_FAILURE, GLC_FAIL_NON_FINITE);
@@ -685,31 +684,22 @@ struct Ray {
       ah += h;
     }
     commit_azimuth(S(x_old), S(y_old), S(yh[0]), S(yh[1]));
-    if (sc.track) update_drifts(o.inv);
+    if (sc.track) {
+      if (pair) {
+        // L_z and Carter's constant from the committed pair state, on accepted steps only
+        Invariants<C> inv = o.inv;
+        pair_invariants(inv);
+        update_drifts(inv);
+      } else {
+        update_drifts(o.inv);
+      }
+    }
     for (int c = 0; c < 7; ++c) k1[c] = o.k7[c];
     r = o.r_end;
     vr = o.vr_end;
     arm_update(sc, pol);
     h = dir * next_step(pol, g_abs(h), o.en, true);
     (void)stepped64;
-  }
-
-  GLC_HD void pair_invariants_after(StepOut& o) const {
-    if constexpr (kPair) {
-      // L from the end-of-step pair state (compensated products)
-      C hh[6], ll[6];
-      for (int c = 0; c < 6; ++c) {
-        hh[c] = yh[c];
-        ll[c] = yl[c];
-        ff_add_any(hh[c], ll[c], o.inc[c]);
-      }
-      const float lx = ff_cross(hh[1], ll[1], hh[5], ll[5], hh[2], ll[2], hh[4], ll[4]);
-      const float ly = ff_cross(hh[2], ll[2], hh[3], ll[3], hh[0], ll[0], hh[5], ll[5]);
-      o.inv.lz = ff_cross(hh[0], ll[0], hh[4], ll[4], hh[1], ll[1], hh[3], ll[3]);
-      o.inv.carter = lx * lx + ly * ly + o.inv.abracket;
-    } else {
-      (void)o;
-    }
   }
 
   GLC_HD void arm_update(const LaneScene& sc, const glc_policy& pol) {
