@@ -71,8 +71,13 @@ struct PrecTraits<kTAIL> {
 // BULK hands a surface crossing to TAIL when its binary32 root radius lies within this relative
 // margin of the surface's radial interval, so that TAIL's binary64 root decides hits near the edges.
 constexpr double kBulkSurfaceMargin = 1e-4;
-// BULK localizes its non-terminal roots (radial turning points, equatorial crossings off the
-// surface) to at least this affine tolerance: binary32 cannot resolve the binary64 presets' 2e-11.
+// A surface crossing whose step keeps the sign of its radial velocity, and whose end radii both lie
+// outside the surface's radial interval widened by this relative margin (on the same side), misses
+// the surface: it is decided without its root, in every precision.
+constexpr double kSurfaceMissMargin = 1e-4;
+// BULK localizes its non-terminal roots (pericentres, for the turning radius, and surface crossings
+// near the surface) to at least this affine tolerance: binary32 cannot resolve the binary64
+// presets' 2e-11.
 constexpr double kBulkRootTolerance = 1e-6;
 
 enum EventBit : uint32_t { kEvGuard = 0, kEvHorizon = 1, kEvSurface = 2, kEvEscape = 3 };
@@ -730,6 +735,33 @@ struct Ray {
   // commits the step as a plain one.
   GLC_HD bool event_path(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, const StepOut& o) {
     using T = S;
+    uint32_t mask = o.mask;
+    {
+      // Decisions without the dense output. Outside the horizon a null geodesic's r has at most one
+      // turning point, so on a step whose radial velocity keeps its sign r moves monotonically
+      // between the end radii, and a surface crossing's radius lies between them: when both lie
+      // outside the surface's radial interval (widened by the margin, on the same side), the
+      // crossing misses the surface. Otherwise its root decides, below.
+      const bool turning = (mask >> 4) & 1u;
+      if (((mask >> kEvSurface) & 1u) && !turning) {
+        const double lo = g_min(double(r), double(o.r_end)), hi = g_max(double(r), double(o.r_end));
+        if (hi < sc.surf_in * (1.0 - kSurfaceMissMargin) || lo > sc.surf_out * (1.0 + kSurfaceMissMargin))
+          mask &= ~(1u << kEvSurface);
+      }
+      if ((mask & 0xFu) == 0u) {
+        // No event root in the step, so nothing to order the crossings and turnings against. An
+        // equatorial crossing's root always exists on the dense output (z changes sign between its
+        // ends), so it is counted without localizing it.
+        if ((mask >> 5) & 1u) crossings += 1;
+        mask &= ~(1u << 5);
+        if (!turning) return false;
+        // an outward turning (apocentre) is counted likewise; a pericentre's radius needs its root
+        if (!(dir * vr < C(0) && dir * o.vr_end >= C(0))) {
+          turnings += 1;
+          return false;
+        }
+      }
+    }
     const KN<T> kt = kn_cast<T>(sc.kn);
     T y[6];
     state_s(y);
@@ -757,7 +789,7 @@ struct Ray {
     T thetas[4], residuals[4], states[4][6];
     for (int kind = 0; kind < 4; ++kind) {
       if (P == kBULK && kind != kEvSurface) continue;  // the other events were handed off already
-      if (!((o.mask >> kind) & 1u)) continue;
+      if (!((mask >> kind) & 1u)) continue;
       const T sv = T(event_value<C>(kind, sc, guard, r, o.z0));
       const T evv = T(event_value<C>(kind, sc, guard, o.r_end, o.z1));
       T th_, yr[6], br;
@@ -807,7 +839,7 @@ struct Ray {
     // the replaced GPU kernel's gate: the terminal inside a turning point's root bracket
     bool turning_uncertain = false;
     // radial turning point (geodesic.rs:330-360)
-    if ((o.mask >> 4) & 1u) {
+    if ((mask >> 4) & 1u) {
       const T sv = T(dir * vr), evv = T(dir * o.vr_end);
       T th_, yr[6], br;
       auto vr_at = [&](const T* ys_, T& v) -> bool {
@@ -829,7 +861,7 @@ struct Ray {
       if (has_event && (!found || g_abs(th_ - term_theta) * g_abs(hh) <= br)) turning_uncertain = true;
     }
     // equatorial crossing (geodesic.rs:362-383)
-    if ((o.mask >> 5) & 1u) {
+    if ((mask >> 5) & 1u) {
       T th_, yr[6], br;
       auto z_at = [&](const T* ys_, T& v) -> bool {
         v = ys_[2];
