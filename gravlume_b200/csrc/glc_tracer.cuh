@@ -22,6 +22,7 @@
 //          shell steps, observables and the null-constraint renormalisation).
 #pragma once
 
+#include <cfloat>
 #include <type_traits>
 
 // Form of the DP5(4) attempt: 0 fully unrolled stages; 1 one rolled loop over a stage array (local
@@ -966,10 +967,15 @@ struct Ray {
 //   d[0..5] the state (x, y, z, p_x, p_y, p_z) in binary64 (the sum of the compensated pair),
 //   d[6] the affine parameter, d[7] the coordinate-time increment sum;
 //   f[0..7] step size with direction, L_z and Carter's constant at the start, minimum turning radius,
-//   the null residual, L_z and Carter drift maxima, unused;
+//   the null residual, L_z and Carter drift maxima, and the radius at the state as BULK's last
+//   crossing checks saw it;
 //   u[0..7] accepted, rejected, consecutive rejects, armed event bits, radial turnings, equatorial
 //   crossings, winding, and polar side + 1 | flags << 4 | termination << 16 | failure << 24 |
+//   sign of the radial velocity at the state (0 positive, 1 negative, 2 zero) << 28 |
 //   invariants valid << 31.
+// The radius and the sign of the radial velocity carry BULK's sign chain over to TAIL: the state's
+// binary64 values can fall on the other side of an event (a state a few binary32 ulps inside the
+// escape sphere whose binary64 radius is already outside it would never see the sphere crossed).
 // E, the initial azimuth and the direction are not stored: TAIL re-derives them from the ray's
 // initial state, exactly as BULK did.
 struct alignas(16) HandoffRec {
@@ -990,7 +996,7 @@ GLC_HD void handoff_pack(const Ray<kBULK>& ray, const RayResult<float>& res, Han
   rec.f[4] = ray.dnull;
   rec.f[5] = ray.dlz;
   rec.f[6] = ray.dq;
-  rec.f[7] = 0.0f;
+  rec.f[7] = ray.r;
   rec.u[0] = ray.accepted;
   rec.u[1] = ray.rejected;
   rec.u[2] = ray.consecutive;
@@ -999,7 +1005,8 @@ GLC_HD void handoff_pack(const Ray<kBULK>& ray, const RayResult<float>& res, Han
   rec.u[5] = ray.crossings;
   rec.u[6] = uint32_t(ray.winding);
   rec.u[7] = uint32_t(ray.polar + 1) | ((ray.flags & 0xFFFu) << 4) | ((res.termination & 0xFFu) << 16) |
-             ((res.failure & 0xFu) << 24) | (ray.have_inv ? 1u << 31 : 0u);
+             ((res.failure & 0xFu) << 24) | (ray.vr < 0.0f ? 1u << 28 : (ray.vr == 0.0f ? 2u << 28 : 0u)) |
+             (ray.have_inv ? 1u << 31 : 0u);
 }
 
 // Resume a handed-off ray as a binary64 stepper: the stored state and counters, E and the initial
@@ -1040,8 +1047,14 @@ GLC_HD uint32_t handoff_unpack(const HandoffRec& rec, Ray<kTAIL>& ray, const Lan
   failure = (w >> 24) & 0xFu;
   double rr, vv;
   kn_rhs(sc.kn, ray.yh, ray.Ec, ray.k1, rr, vv);
-  ray.r = rr;
+  // continue BULK's sign chain: its radius at the state, and a radial velocity of its sign
+  ray.r = double(rec.f[7]);
+  const uint32_t vs = (w >> 28) & 3u;
+  if (vs == 2u) vv = 0.0;
+  else if (vs == 1u && !(vv < 0.0)) vv = -DBL_MIN;
+  else if (vs == 0u && !(vv > 0.0)) vv = DBL_MIN;
   ray.vr = vv;
+  (void)rr;
   return (w >> 16) & 0xFFu;
 }
 

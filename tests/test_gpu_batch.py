@@ -157,6 +157,12 @@ def test_mixed_work_queue_kernels_run_the_two_kernel_form(pipe, job, persistent)
     queued = trace(pipe, scenes, cams, slots)
     assert pipe.stats().last_persistent == persistent
     assert np.all(queued["f64_steps"][queued["flags"] & 0x30 == 0] >= 1), "every integrated ray was completed"
+    # every ray of the batch ends by an event: none may run to the step or reject caps, which is
+    # what a completion that misses the event the bulk kernel handed over for would do
+    for d in (simple, queued):
+        assert not np.any(np.isin(d["termination"], [G.Termination.STEP_EXHAUSTION, G.Termination.REJECT_EXHAUSTION]))
+    steps = lambda d: d["accepted_steps"].astype(np.int64) + d["rejected_steps"]
+    assert steps(queued).max() <= 2 * steps(simple).max()
     n = slots
     assert np.count_nonzero(queued["termination"] != simple["termination"]) <= max(1, n // 100000)
     same = queued["termination"] == simple["termination"]

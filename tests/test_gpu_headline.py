@@ -2,7 +2,7 @@
 observer at r = 50 M and inclination 75 deg, pinhole 3840x2160 with a 30 deg vertical field of view,
 escape at 1000 M, capture at r_+ + 1e-3, Keplerian surface from the prograde ISCO to 20 M.
 
-2048 seeded pixels are traced by the oracle at rtol 1e-10 / atol 1e-12 and compared with the whole
+4096 seeded pixels are traced by the oracle at rtol 1e-10 / atol 1e-12 and compared with the whole
 CUDA frame in FP32, MIXED (two kernels, the default, and one kernel) and FP64:
   - termination classes are identical outside the near-critical band. The band is the set of
     sampled rays whose oracle answer moves when the oracle's own tolerance is loosened to
