@@ -33,11 +33,12 @@ SPIN, CHARGE, INCL_DEG, R_OBS, FOV_DEG = 0.9, 0.3, 75.0, 50.0, 30.0
 ESCAPE, HORIZON_OFFSET, SURFACE_OUTER = 1000.0, 1e-3, 20.0
 METRIC = "Mrays/s at 3840x2160 a=0.9, mixed vs plain at equal FP64 error; adjoint Mrays/s"
 L2_BYTES = 126 * 2 ** 20
-# DRAM bytes (read + write) per ray of the trace kernel from the committed ncu captures of the same
-# scene at 1280x720 (profiles/trace_simple_kernel_{mixed,fp32,fp64}_1280x720_full.md): the result
-# stores (200 B/ray, part of which the 126 MB L2 still holds when a 720p launch ends), scaled by the
-# ray count.
-TRAFFIC_BYTES_PER_RAY = {"mixed": (3.697920e6 + 139.899904e6) / 921600, "fp32": (3.149056e6 + 146.922240e6) / 921600,
+# DRAM bytes (read + write) per ray of the frame's kernels from ncu captures of the same scene at
+# 1280x720 (the bulk and tail kernels; the one-kernel FP32 and FP64), scaled by the ray count. MIXED is the
+# bulk and tail kernels together: the 128-byte hand-off record written and read back, and the
+# 200-byte results (part of each still in the 126 MB L2 when a 720p launch ends).
+TRAFFIC_BYTES_PER_RAY = {"mixed": (0.170496e6 + 60.292352e6 + 119.521536e6 + 140.539392e6) / 921600,
+                         "fp32": (3.495936e6 + 145.957632e6) / 921600,
                          "fp64": (8.472576e6 + 141.483776e6) / 921600}
 
 
@@ -410,7 +411,7 @@ def run_gpu(args) -> None:
                 "flops_per_attempt": float(flops[2]),
                 "traffic": args.traffic_bytes if args.traffic_bytes is not None else (
                     TRAFFIC_BYTES_PER_RAY[args.precision] * rays_here if args.precision in TRAFFIC_BYTES_PER_RAY else None),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1280x720, scaled by rays",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the frame's kernels at 1280x720, scaled by rays",
                 "algorithmic_bytes_per_launch": float(sum(N.RESULT_BYTES.values())) * rays_here}
     # the same launch against HBM, to show how far from bandwidth-bound the path is
     hbm_peak, hbm_source = 6650.0, "fallback"

@@ -204,8 +204,9 @@ def test_policy_presets_follow_the_reference_and_validate():
 
 
 def test_integration_binding_sizes_match_the_abi():
-    """The Rust binding in INTEGRATION.md declares opaque structs by byte size; those sizes are the
-    C ABI's (as mirrored by the ctypes declarations)."""
+    """The Rust binding that the integration guide at the repository root gives maintainers declares
+    opaque structs by byte size; those sizes are the C ABI's (as mirrored by the ctypes
+    declarations)."""
     import ctypes
     import re
     from pathlib import Path
