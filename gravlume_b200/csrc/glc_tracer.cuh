@@ -761,6 +761,16 @@ struct Ray {
           turnings += 1;
           return false;
         }
+        // MIXED's bulk kernel: the pericentre's radius from the radial potential instead of the
+        // dense output. FP32 and FP64 keep the reference's root on the dense output: they follow
+        // its algorithm wherever a shortcut would change a result, and this one moves the radius
+        // by the drift of the constants of motion.
+        C rp;
+        if (P == kBULK && pericentre_radius(sc, o, rp)) {
+          turnings += 1;
+          turn_r = (turn_r == turn_r) ? g_min(turn_r, rp) : rp;
+          return false;
+        }
       }
     }
     const KN<T> kt = kn_cast<T>(sc.kn);
@@ -897,6 +907,44 @@ struct Ray {
       if ((cand & (cand - 1u)) != 0u || turning_uncertain || drift) res.termination = GLC_TERM_UNCERTAIN;
     }
     return true;
+  }
+
+  // The radius of a pericentre inside the step, as the largest root of the radial potential
+  //   R(r) = [E (r^2 + a^2) - a L_z]^2 - Delta [(L_z - a E)^2 + Q],  Delta = r^2 - 2 r + a^2 + Q_e^2
+  // of the constants of motion at the step's start (Carter's Q in the same L-form as the drift
+  // diagnostics). Outside the horizon the pericentre is R's largest root and lies below both end
+  // radii, where R is positive and rising, so Newton's method from the smaller end radius descends
+  // onto it. It takes a few binary32 evaluations where localizing the root of the radial velocity
+  // on the dense output takes the step's six stages again and a right-hand side per iteration. The
+  // radius differs from that root's by the drift of the constants (the frame tolerance's level).
+  // Returns false when Newton does not settle below the end radii, as near a double root (a ray
+  // grazing the photon orbit); the caller then localizes the root.
+  GLC_HD bool pericentre_radius(const LaneScene& sc, const StepOut& o, C& rp) const {
+    const C x = yh[0], y = yh[1], z = yh[2], px = yh[3], py = yh[4], pz = yh[5];
+    const C a = C(sc.kn.a), a2 = C(sc.kn.a2), q2 = C(sc.kn.q2), E = Ec;
+    const C L = x * py - y * px;
+    const C Lx = y * pz - z * py, Ly = z * px - x * pz;
+    const C r0 = r, r02 = r0 * r0;
+    const C Q = Lx * Lx + Ly * Ly +
+                a2 * (z * z / r02 * (px * px + py * py - E * E) - (x * x + y * y) / (r02 + a2) * pz * pz);
+    const C K = (L - a * E) * (L - a * E) + Q;
+    const C top = g_min(r0, C(o.r_end));
+    C rr = top;
+    for (int it = 0; it < 16; ++it) {
+      const C w = E * (rr * rr + a2) - a * L;
+      const C R = w * w - (rr * rr - C(2) * rr + a2 + q2) * K;
+      const C dR = C(4) * E * rr * w - (C(2) * rr - C(2)) * K;
+      if (!(dR > C(0))) return false;
+      const C step = R / dR;
+      rr -= step;
+      if (!(rr > C(0.5) * top)) return false;
+      if (g_abs(step) <= C(1e-7) * rr) {
+        if (!(rr <= top * C(1.000001))) return false;
+        rp = rr;
+        return true;
+      }
+    }
+    return false;
   }
 
   // BULK: leave the ray to TAIL at the current state (termination NONE: not finished).
