@@ -746,8 +746,15 @@ struct Ray {
       const bool turning = (mask >> 4) & 1u;
       if (((mask >> kEvSurface) & 1u) && !turning) {
         const double lo = g_min(double(r), double(o.r_end)), hi = g_max(double(r), double(o.r_end));
-        if (hi < sc.surf_in * (1.0 - kSurfaceMissMargin) || lo > sc.surf_out * (1.0 + kSurfaceMissMargin))
+        if (hi < sc.surf_in * (1.0 - kSurfaceMissMargin) || lo > sc.surf_out * (1.0 + kSurfaceMissMargin)) {
           mask &= ~(1u << kEvSurface);
+        } else if (P == kBULK && lo > sc.surf_in * (1.0 + kBulkSurfaceMargin) &&
+                   hi < sc.surf_out * (1.0 - kBulkSurfaceMargin)) {
+          // BULK: the crossing lies on the surface, away from its edges, so TAIL takes the step
+          // (the binary32 root would only confirm the hand-off)
+          accepted -= 1;
+          return hand_off(res);
+        }
       }
       if ((mask & 0xFu) == 0u) {
         // No event root in the step, so nothing to order the crossings and turnings against. An
