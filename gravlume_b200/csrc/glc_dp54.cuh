@@ -252,8 +252,12 @@ GLC_HD C dp5_attempt_compact(const KN<C>& k, const S y0[6], C E, C h, const C k1
 template <class C, class S, bool kInv = true, bool kFold = std::is_same<C, double>::value>
 GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start, const Tolerance& tol,
                             C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite,
-                            bool track = true) {
+                            bool track = true, C (*stages)[7] = nullptr) {
   using Coef = StreamCoef<C>;
+  // stages (optional): the seven stage derivatives of this attempt, for a dense output built
+  // without evaluating them again
+  if (stages != nullptr)
+    for (int c = 0; c < 7; ++c) stages[0][c] = k1[c];
   C y0c[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) y0c[c] = C(y0[c]);
@@ -283,6 +287,8 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
     } else {
       kn_rhs<C, false>(k, ys, E, d, rr, vv);
     }
+    if (stages != nullptr)
+      for (int c = 0; c < 7; ++c) stages[j][c] = d[c];
     // pending sums of the stages still ahead (stage j + 2 + m <= 7); the rest would only add
     // zero coefficients
 #pragma unroll
@@ -303,6 +309,8 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
       ys[c] = y0c[c] + inc[c];
     }
     kn_rhs<C, kInv>(k, ys, E, d, rr, vv, track ? &inv : nullptr);
+    if (stages != nullptr)
+      for (int c = 0; c < 7; ++c) stages[6][c] = d[c];
 #pragma unroll
     for (int c = 0; c < 7; ++c) err[c] += Coef::e(6) * d[c];
   }

@@ -510,7 +510,9 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks)
   if (term != GLC_TERM_NONE) {
     ray.finish_plain(res, term, failure);
   } else {
-    while (!ray.step(ls, pol, res, false)) {
+    // the stages of each attempt, kept (in local memory) for the terminal step's dense output
+    double stages[7][7];
+    while (!ray.step(ls, pol, res, false, stages)) {
     }
   }
   write_result<kTAIL>(out, slot, ray, res, ls);

@@ -578,7 +578,11 @@ struct Ray {
   // Advance by one attempted step. Returns true when the ray terminated (result filled). use64
   // (MIXED only): take this step in binary64 (the warp has a lane inside the shell). One step body
   // serves both cases; only the attempt itself branches.
-  GLC_HD bool step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, bool use64) {
+  // stages (optional, binary64 stepping only): where the attempt leaves its seven stage
+  // derivatives, so that the event path builds the dense output from them instead of evaluating
+  // the stages again
+  GLC_HD bool step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, bool use64,
+                   C (*stages)[7] = nullptr) {
     if (uint64_t(accepted) >= pol.maximum_accepted_steps) {
       finish_plain(res, GLC_TERM_STEP_EXHAUSTION, GLC_FAIL_NONE);
       return true;
@@ -613,7 +617,7 @@ struct Ray {
                                              o.inv, finite);
 #elif GLC_ATTEMPT_FORM == 2
       o.en = dp5_attempt_stream<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
-                                            o.inv, finite, sc.track);
+                                            o.inv, finite, sc.track, stages);
 #else
       o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
                                      finite);
@@ -672,7 +676,7 @@ struct Ray {
       o.stepped64 = stepped64;
       // inline: with the streaming attempt the ray fits in registers, and copying it to local
       // memory for an out-of-line call measured 12-15 % slower in every precision
-      if (event_path(sc, pol, res, o)) return true;
+      if (event_path(sc, pol, res, o, stages)) return true;
     }
     commit(sc, pol, o, stepped64);
     return false;
@@ -734,7 +738,8 @@ struct Ray {
   // polynomial from the stepping-precision stages), events are ordered and, for a terminal event,
   // the observables are evaluated in S. Returns true when the ray terminated; otherwise the caller
   // commits the step as a plain one.
-  GLC_HD bool event_path(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, const StepOut& o) {
+  GLC_HD bool event_path(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, const StepOut& o,
+                         const C (*stages)[7] = nullptr) {
     using T = S;
     uint32_t mask = o.mask;
     {
@@ -785,7 +790,9 @@ struct Ray {
     state_s(y);
     // stages for the dense output, in the stepping precision (binary64 on MIXED shell steps)
     DensePoly<T> dpoly;
-    if (o.stepped64) {
+    if (stages != nullptr) {
+      dpoly.build(stages);
+    } else if (o.stepped64) {
       double K[7][7], yk[6], rr, vv, ye[6];
       for (int c = 0; c < 6; ++c) yk[c] = double(y[c]);
       kn_rhs(sc.kn, yk, double(E), K[0], rr, vv);
