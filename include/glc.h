@@ -165,12 +165,17 @@ typedef struct glc_policy {
                                      cameras of surface-free scenes; certified rays skip integration */
   uint32_t escape_map;            /* 1: escape-direction map (node pass on every 4th pixel, stable
                                      8x8 tiles of surface-free scenes reconstructed by interpolation) */
-  uint32_t mixed_split;           /* MIXED with persistent = 0: 1 (default) two kernels, binary32
-                                     stepping with the pair state until a ray's first step that
-                                     brackets a terminal event or enters the shell, then binary64
-                                     from a 128-byte hand-off record per ray (context memory,
-                                     grow-only); 0: one kernel whose warps step in binary64 while
-                                     a lane is inside the shell */
+  uint32_t mixed_split;           /* MIXED: 1 (default) two kernels, binary32 stepping with the
+                                     pair state (in the one-thread-per-ray kernel or either work
+                                     queue) until a ray's first step that brackets a terminal
+                                     event, crosses the surface near or on it, or enters the shell,
+                                     then binary64 from a 128-byte hand-off record per ray (context
+                                     memory, grow-only). The binary32 stepping takes a pericentre's
+                                     turning radius as the largest root of the radial potential of
+                                     the step's constants of motion rather than the root of the
+                                     radial velocity on the dense output (the two differ by the
+                                     constants' drift). 0: one kernel whose warps step in binary64
+                                     while a lane is inside the shell */
   uint32_t uncertain_terminals;   /* 1: the replaced wgpu kernel's gate (geodesic_integration.wgsl
                                      324-330): a terminal becomes GLC_TERM_UNCERTAIN when more than
                                      one event lies within the tie tolerance of the earliest, when
