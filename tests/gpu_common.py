@@ -103,6 +103,14 @@ def compare(gpu: dict, sel: np.ndarray, ref: np.ndarray) -> dict:
         rep["radial_turnings_mismatch"] = int((gpu["radial_turnings"][sel][same] != ref[same, F["radial_turnings"]]).sum())
         rep["equatorial_crossings_mismatch"] = int(
             (gpu["equatorial_crossings"][sel][same] != ref[same, F["equatorial_crossings"]]).sum())
+        if "has_turning_radius" in gpu:
+            gh = gpu["has_turning_radius"][sel][same] == 1
+            oh = ref[same, F["has_turning_radius"]] == 1
+            rep["has_turning_mismatch"] = int((gh != oh).sum())
+            both = gh & oh
+            if both.any():
+                otr = ref[same, F["turning_radius"]][both]
+                rep["turning_radius_rel"] = float(np.max(np.abs(gpu["turning_radius"][sel][same][both] - otr) / otr))
     return rep
 
 

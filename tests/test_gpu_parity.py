@@ -71,6 +71,7 @@ def test_fp64_image_matches_the_oracle_on_every_config1_pixel(pipe, config1_orac
         if k in rep:
             assert rep[k] <= tol, (k, rep)
     assert rep["radial_turnings_mismatch"] == 0 and rep["equatorial_crossings_mismatch"] == 0
+    assert rep["has_turning_mismatch"] == 0 and rep["turning_radius_rel"] <= 1e-8, rep
 
 
 # The same frame policy over every pixel of the frame outside the near-critical band: the largest
@@ -118,7 +119,9 @@ CONFIG2_SCENES = [(a, q, i) for a, q in ((0.0, 0.0), (0.5, 0.0), (0.9, 0.3), (0.
 def test_full_frame_scene_set_matches_the_oracle(pipe, a, q, incl):
     """The full-frame precision set at 1920x1080: each of the 15 scenes in FP32, MIXED and FP64 at
     the frame tolerance against 128 seeded oracle rays at rtol 1e-10; classes identical outside the
-    near-critical band (as for the 256x256 frame), observables within the frame budgets."""
+    near-critical band (as for the 256x256 frame), observables within the frame budgets, and the
+    pericentre radius (localized on the dense output in FP32 and FP64, from the radial potential
+    in MIXED's binary32 stepping) within 1e-4 of the oracle's."""
     w, h = 1920, 1080
     obs = config1_observation(width=w, height=h, spin=a, charge=q, incl_deg=incl)
     osc, ev, _ = oracle_for(obs)
@@ -137,6 +140,8 @@ def test_full_frame_scene_set_matches_the_oracle(pipe, a, q, incl):
         for k, tol in F32_BUDGET.items():
             if k in rep:
                 assert rep[k] <= tol, (precision.name, k, rep)
+        assert rep.get("has_turning_mismatch", 0) == 0, (precision.name, rep)
+        assert rep.get("turning_radius_rel", 0.0) <= 1e-4, (precision.name, rep)
 
 
 def test_persistent_and_simple_kernels_agree(pipe):
