@@ -249,7 +249,10 @@ GLC_HD C dp5_attempt_compact(const KN<C>& k, const S y0[6], C E, C h, const C k1
 // loop's instruction footprint is about a sixth of the unrolled form's.
 // kFold: the end-point evaluation is the loop's sixth pass (one right-hand-side body; measured
 // faster in binary64) or follows the loop as its own call (measured faster in binary32).
-template <class C, class S, bool kInv = true, bool kFold = std::is_same<C, double>::value>
+// kUnroll: the stage loop unrolled (the binary32 bulk kernel of MIXED, whose instruction footprint
+// is small enough that the coefficients as immediates pay) or rolled (1; every other kernel, where
+// the unrolled footprint measured slower: instruction fetch).
+template <class C, class S, bool kInv = true, bool kFold = std::is_same<C, double>::value, int kUnroll = 1>
 GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[7], C t_start, const Tolerance& tol,
                             C inc[6], C& dt, C k7[7], C& r_end, C& vr_end, Invariants<C>& inv, bool& finite,
                             bool track = true, C (*stages)[7] = nullptr) {
@@ -271,7 +274,7 @@ GLC_HD C dp5_attempt_stream(const KN<C>& k, const S y0[6], C E, C h, const C k1[
   bt = Coef::b(0) * k1[6];
   C ys[6], rr = C(0), vv = C(0), d[7];
   constexpr int kPasses = kFold ? 7 : 6;
-#pragma unroll 1
+#pragma unroll kUnroll
   for (int j = 1; j < kPasses; ++j) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) {

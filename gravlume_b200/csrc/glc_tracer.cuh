@@ -616,8 +616,11 @@ struct Ray {
       o.en = dp5_attempt_compact<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
                                              o.inv, finite);
 #elif GLC_ATTEMPT_FORM == 2
-      o.en = dp5_attempt_stream<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end,
-                                            o.inv, finite, sc.track, stages);
+      // MIXED's bulk kernel unrolls the stage loop (+5 % there; the one-kernel FP32 lost 13 % with
+      // it, to instruction fetch)
+      constexpr int kUnroll = P == kBULK ? 6 : 1;
+      o.en = dp5_attempt_stream<C, C, true, std::is_same<C, double>::value, kUnroll>(
+          kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv, finite, sc.track, stages);
 #else
       o.en = dp5_attempt<C, C, true>(kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv,
                                      finite);
