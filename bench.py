@@ -37,7 +37,7 @@ L2_BYTES = 126 * 2 ** 20
 # 1280x720 (the bulk and tail kernels; the one-kernel FP32 and FP64), scaled by the ray count. MIXED is the
 # bulk and tail kernels together: the 128-byte hand-off record written and read back, and the
 # 200-byte results (part of each still in the 126 MB L2 when a 720p launch ends).
-TRAFFIC_BYTES_PER_RAY = {"mixed": (0.115712e6 + 62.366464e6 + 119.667456e6 + 162.029056e6) / 921600,
+TRAFFIC_BYTES_PER_RAY = {"mixed": (0.093696e6 + 62.725632e6 + 120.360704e6 + 160.456704e6) / 921600,
                          "fp32": (3.284480e6 + 146.337792e6) / 921600,
                          "fp64": (8.472576e6 + 141.483776e6) / 921600}
 
