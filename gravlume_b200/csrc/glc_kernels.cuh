@@ -385,7 +385,8 @@ struct LaunchShape {
 template <int P>
 __device__ __forceinline__ bool ray_step(Ray<P>& ray, const LaneScene& ls, const glc_policy& pol,
                                          RayResult<typename PrecTraits<P>::S>& res, bool use64) {
-  return ray.step(ls, pol, res, P == kMIXED && use64);
+  // rolled stage loop: the work-queue kernels and the one-kernel modes
+  return ray.template step<1>(ls, pol, res, P == kMIXED && use64);
 }
 
 // One ray from set-up to result (the body of the one-thread-per-ray kernels).
@@ -458,6 +459,7 @@ __device__ __forceinline__ uint32_t handoff_resume(const Handoff& hv, unsigned l
 // or when it enters the binary64 shell, or when it fails, by storing its hand-off record.
 // Certified and map-reconstructed pixels are written here. bulk_one is one ray of it, shared by
 // the one-thread-per-ray kernel and the work-queue kernels.
+template <int kUnroll = 6>
 __device__ __forceinline__ void bulk_one(const JobView& job, const glc_policy& pol, const glc_results& out,
                                          const Handoff& hv, unsigned long long gi) {
   if (gi >= job.total) return;
@@ -475,7 +477,7 @@ __device__ __forceinline__ void bulk_one(const JobView& job, const glc_policy& p
   Ray<kBULK> ray;
   ray.init(ls, pol, st8, dir);
   RayResult<float> res;
-  while (!ray.step(ls, pol, res, false)) {
+  while (!ray.template step<kUnroll>(ls, pol, res, false)) {
   }
   handoff_store(hv, gi, ray, res);
 }
@@ -536,7 +538,7 @@ __global__ void __launch_bounds__(128, LaunchShape<P>::kMinBlocks) trace_queue_k
     base = __shfl_sync(FULL, base, 0);
     if (base >= job.total) break;
     for (unsigned k = 0; k < grab; k += 32u) {
-      if constexpr (P == kBULK) bulk_one(job, pol, out, hv, base + k + lane);
+      if constexpr (P == kBULK) bulk_one<1>(job, pol, out, hv, base + k + lane);
       else trace_one<P>(job, pol, out, base + k + lane);
     }
   }

@@ -581,6 +581,9 @@ struct Ray {
   // stages (optional, binary64 stepping only): where the attempt leaves its seven stage
   // derivatives, so that the event path builds the dense output from them instead of evaluating
   // the stages again
+  // kUnroll: the attempt's stage loop unrolled (6) or rolled (1); unrolled by default only in
+  // MIXED's bulk stepping, whose small footprint lets it pay.
+  template <int kUnroll = (P == kBULK ? 6 : 1)>
   GLC_HD bool step(const LaneScene& sc, const glc_policy& pol, RayResult<S>& res, bool use64,
                    C (*stages)[7] = nullptr) {
     if (uint64_t(accepted) >= pol.maximum_accepted_steps) {
@@ -617,8 +620,7 @@ struct Ray {
                                              o.inv, finite);
 #elif GLC_ATTEMPT_FORM == 2
       // MIXED's bulk kernel unrolls the stage loop (+5 % there; the one-kernel FP32 lost 13 % with
-      // it, to instruction fetch)
-      constexpr int kUnroll = P == kBULK ? 6 : 1;
+      // it, to instruction fetch, and so did the work-queue kernels, which inline it into more code)
       o.en = dp5_attempt_stream<C, C, true, std::is_same<C, double>::value, kUnroll>(
           kc, yh, Ec, h, k1, th + tl, tol, o.inc, o.dt, o.k7, o.r_end, o.vr_end, o.inv, finite, sc.track, stages);
 #else
