@@ -16,10 +16,15 @@
 //   MIXED: S = double, C = float; a warp whose lanes are inside the shell r < shell radius steps
 //          in double; the event path and the final null-constraint renormalisation are double.
 //   MIXED as two kernels (the frame path): BULK steps in binary32 with the compensated pair state
-//          (S = C = float) and leaves a ray at its first step that brackets a terminal event, or
-//          when it enters the shell; TAIL (S = C = double) resumes the ray from its hand-off
-//          record, re-takes that step, and finishes the trace in binary64 (event root-finding,
-//          shell steps, observables and the null-constraint renormalisation).
+//          (S = C = float) and leaves a ray at its first step that brackets a terminal event or
+//          crosses the surface near or on it, or when it enters the shell; TAIL (S = C = double)
+//          resumes the ray from its hand-off record, re-takes that step, and finishes the trace
+//          in binary64 (event root-finding, shell steps, observables and the null-constraint
+//          renormalisation). BULK counts crossings and turnings without roots where no event
+//          root shares the step, and takes a pericentre's radius from the radial potential.
+// In every mode, a step with no event root counts its equatorial crossing and an apocentre from
+// the sign changes alone (their roots always exist on the dense output), and a surface crossing
+// whose end radii both lie clear of the surface's radial interval is a miss without a root.
 #pragma once
 
 #include <cfloat>
