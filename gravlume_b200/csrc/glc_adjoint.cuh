@@ -174,11 +174,37 @@ GLC_HD void stages_reverse(const KN<Dual<4, R>>& kd, const double Y[7][6], doubl
 
 // Adjoint of one accepted step from y0 with size h (stage points recomputed in binary64, the stage
 // products in the scalar type of kd).
+// Stage points of the step in binary32, as the MIXED forward pass formed them (from the binary32
+// high part of its state): the dual products that follow are binary32 anyway.
+GLC_HD void dp5_stage_points_f32(const KN<double>& k, const double y0[6], double E, double h, double Y[7][6]) {
+  const KN<float> kf = kn_cast<float>(k);
+  const float hf = float(h), Ef = float(E);
+  float y0f[6], K[7][6];
+  for (int c = 0; c < 6; ++c) y0f[c] = float(y0[c]);
+  for (int i = 0; i < 7; ++i) {
+    float ys[6];
+    for (int c = 0; c < 6; ++c) {
+      float s = 0.0f;
+      for (int j = 0; j < i; ++j) s += dp_a<float>(i, j) * K[j][c];
+      ys[c] = y0f[c] + hf * s;
+      Y[i][c] = double(ys[c]);
+    }
+    float d[7], r, vr;
+    kn_rhs(kf, ys, Ef, d, r, vr);
+    for (int c = 0; c < 6; ++c) K[i][c] = d[c];
+  }
+}
+
 template <class R>
 GLC_HD void dp5_reverse(const KN<double>& k, const KN<Dual<4, R>>& kd, const double y0[6], double E, double h,
                         const double w[7], const double lam[6], double lam0[6], double g[3]) {
-  double Y[7][6], K[7][6];
-  dp5_stage_points(k, y0, E, h, Y, K);
+  double Y[7][6];
+  if constexpr (std::is_same<R, float>::value) {
+    dp5_stage_points_f32(k, y0, E, h, Y);
+  } else {
+    double K[7][6];
+    dp5_stage_points(k, y0, E, h, Y, K);
+  }
   stages_reverse(kd, Y, E, h, w, lam, lam0, g);
 }
 
