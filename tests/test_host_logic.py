@@ -72,6 +72,21 @@ def test_split_mixed_matches_the_oracle(config1_rays):
     assert (d["f64_steps"] >= 1).all()
 
 
+def test_split_mixed_pericentre_radius_matches_the_oracle(config1_rays):
+    """The binary32 bulk stepping takes a pericentre's radius as the largest root of the radial
+    potential of the step's constants of motion (Newton in binary32, with the dense-output root as
+    the fallback): on the host-compiled kernel logic it has a pericentre exactly where the oracle
+    has one, within 1e-5 of the oracle's radius."""
+    sc, states, ref = config1_rays
+    d = H.trace_split(sc, G.ReferencePolicy.frame(G.Precision.MIXED), states, -1.0)
+    has = ref[:, O.F["has_turning_radius"]] == 1
+    assert np.array_equal(np.isfinite(d["turning_radius"]), has)
+    assert has.sum() >= 10
+    otr = ref[has, O.F["turning_radius"]]
+    rel = np.abs(d["turning_radius"][has] - otr) / otr
+    assert rel.max() <= 1e-5, float(rel.max())
+
+
 def test_split_mixed_equals_one_kernel_mixed_before_the_hand_off(config1_rays):
     """Both MIXED forms step the same binary32 pair state, so they agree to a few binary32 ulps of
     the rtol 1e-6 truncation error on every observable and take the same number of accepted steps
