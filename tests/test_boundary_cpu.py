@@ -216,3 +216,14 @@ def test_integration_binding_sizes_match_the_abi():
     assert sizes["glc_policy"] == ctypes.sizeof(N.Policy)
     assert sizes["glc_scene"] == ctypes.sizeof(N.Scene)
     assert "pub tile_origin: [u32; 2]" in text and ctypes.sizeof(N.Camera) == 80
+
+
+def test_flop_model_counts_the_current_step():
+    """The roofline's algorithmic work unit, counted on the host by instantiating the device
+    templates on a counting scalar: 100 flops and 3 special functions per right-hand side, 1098
+    flops per attempted DP5(4) step (six right-hand sides, the stage combinations, the error norm,
+    the end-point invariants and the controller)."""
+    f = np.zeros(4)
+    assert N.lib().glc_flop_model(f.ctypes.data) == 0
+    assert f[0] == 100.0 and f[1] == 3.0, f
+    assert f[2] == 1098.0, f
